@@ -1,0 +1,195 @@
+/* trav.h -- C ABI of the B200 traversal library (libtrav_b200.so).
+ *
+ * Single-source shortest paths (Bellman-Ford and delta-stepping over the same
+ * relaxation) and breadth-first search (top-down / bottom-up) on one NVIDIA
+ * B200, behind plain C entry points: pointers, sizes and an int status.
+ *
+ * Conventions
+ *  - Every function returns TRAV_OK (0) or a negative TRAV_ERR_* code; the
+ *    message of the last failure on the calling thread is trav_last_error().
+ *  - Vertex ids are int32 in [0, V); edge counts are int64 but a graph must
+ *    hold fewer than 2^31 edges (the device CSR uses int32 offsets).
+ *  - Weights are fp32, finite and >= 0.  Distances are fp32 with FLT_MAX for
+ *    unreachable vertices, exactly as the reference library writes them;
+ *    every result is bit-identical to the reference's CPU Bellman-Ford.
+ *  - BFS levels are int32 hop counts, -1 for unreachable vertices.
+ *  - `mem` arguments say where a buffer lives: TRAV_MEM_HOST (pageable or
+ *    pinned host memory) or TRAV_MEM_DEVICE (CUDA device memory of the
+ *    current device).
+ *  - A graph handle is not thread-safe: use one handle per host thread.
+ *    Each handle owns a CUDA stream; calls return after their work finishes.
+ */
+#ifndef TRAV_H
+#define TRAV_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TRAV_OK 0
+#define TRAV_ERR_BAD_ARG (-1)        /* invalid argument (ids, sizes, weights, options) */
+#define TRAV_ERR_OOM (-2)            /* device or host allocation failed */
+#define TRAV_ERR_OVERFLOW_INT32 (-3) /* graph has 2^31 or more edges */
+#define TRAV_ERR_TIMEOUT (-4)        /* device step budget or bounded wait exhausted */
+#define TRAV_ERR_CUDA (-5)           /* CUDA runtime error */
+#define TRAV_ERR_NO_DEVICE (-6)      /* no usable CUDA device */
+#define TRAV_ERR_IO (-7)             /* file could not be read or written / bad format */
+
+#define TRAV_MEM_HOST 0
+#define TRAV_MEM_DEVICE 1
+
+#define TRAV_SCHEDULE_PLAIN 0   /* Beamer alpha/beta switch; fixed delta */
+#define TRAV_SCHEDULE_LEARNED 1 /* the schedule MLP decides per step */
+
+typedef struct trav_graph trav_graph;
+
+/* Options of a BFS query.  alpha/beta: Beamer's direction-switch constants
+ * (top-down -> bottom-up when frontier out-edges > unvisited out-edges / alpha;
+ * back when the frontier shrinks below V / beta).  force_direction: -1 = use
+ * the schedule, 0 = top-down only, 1 = bottom-up after the first step. */
+typedef struct {
+    int32_t schedule;
+    float alpha;
+    float beta;
+    int32_t force_direction;
+} trav_bfs_opts;
+
+/* Options of an SSSP query.  delta <= 0 or +inf selects Bellman-Ford (one
+ * bucket: every improved vertex is relaxed in the next round); delta > 0
+ * selects delta-stepping with buckets [k*delta, (k+1)*delta) processed in
+ * order.  The distances are the same bits either way. */
+typedef struct {
+    int32_t schedule;
+    float delta;
+} trav_sssp_opts;
+
+/* Per-query record of the most recent query on a handle. */
+typedef struct {
+    int32_t kind;            /* 0 = BFS, 1 = SSSP */
+    int32_t steps;           /* BFS levels expanded / SSSP relaxation rounds */
+    int32_t buckets;         /* SSSP buckets opened (0 for BFS) */
+    int32_t bottom_up_steps; /* BFS steps run bottom-up */
+    int64_t reached;         /* vertices with a finite result */
+    int64_t reached_edges;   /* out-edges of reached vertices */
+    int64_t algorithmic_bytes; /* schedule-independent byte count of the query */
+    float kernel_ms;         /* device time of the query's traversal launch */
+} trav_query_stats;
+
+/* ------------------------------------------------------------------ graphs */
+
+/* Build a device graph from an edge list (src[e] -> dst[e], weight w[e]).
+ * w may be NULL (all weights 1.0).  The device copy is an int32 CSR with
+ * vertices relabelled by out-degree (descending), rows sorted by neighbour,
+ * plus the transposed CSR for bottom-up BFS; results are reported in the
+ * caller's original ids.  Replaces the per-call edge-list upload of
+ * SingleSourceShortestPaths::gpu_bellman_ford (algorithm/sssp/sssp.hpp:219-277)
+ * and BFS::gpu_bfs (algorithm/bfs/bfs.hpp:212-254). */
+int trav_graph_from_edges(int32_t vertices, int64_t edges, const int32_t *src, const int32_t *dst,
+                          const float *w, int32_t mem, trav_graph **out);
+
+/* Generate a seeded RMAT graph directly on the device and build it.  Restates
+ * GraphGenerationAPI::R_MAT_parallel (include/test/generation/
+ * graph_generation_API.hpp:403-484): V = 2^scale, V*avg edges, integer
+ * percent quadrant probabilities a,b,c,d, weights rand_r/RAND_MAX.  Edge e
+ * uses the rand_r stream of `seed` from LCG step 3*(scale+2)*e, so seed 0
+ * equals the reference run with one thread.  If drop_self_loops, loops are
+ * removed (stable).  The edge list is also written to src/dst/w when they
+ * are non-NULL device buffers of V*avg entries; *edges_out gets the count. */
+int trav_graph_rmat(int32_t scale, int32_t avg, int32_t a, int32_t b, int32_t c, int32_t d, uint32_t seed,
+                    int32_t drop_self_loops, int32_t *src, int32_t *dst, float *w, int64_t *edges_out,
+                    trav_graph **out);
+
+int trav_graph_free(trav_graph *g);
+
+int trav_graph_info(const trav_graph *g, int32_t *vertices, int64_t *edges, int32_t *max_out_degree);
+
+/* Copy the device layout to host arrays (any may be NULL): new_of_old[V],
+ * old_of_new[V], out_off[V+1], out_adj[E], out_w[E], in_off[V+1], in_adj[E]. */
+int trav_graph_export(const trav_graph *g, int32_t *new_of_old, int32_t *old_of_new, int32_t *out_off,
+                      int32_t *out_adj, float *out_w, int32_t *in_off, int32_t *in_adj);
+
+/* ----------------------------------------------------------------- queries */
+
+/* BFS levels from each of n sources: levels[q*V + v].  Replaces
+ * BFS::gpu_bfs / bfs_wrapper (algorithm/bfs/bfs.hpp:212-254,
+ * algorithm/bfs/gpu/bfs.cu:43-81), which return only reachability. */
+int trav_bfs(trav_graph *g, const int32_t *sources, int32_t n, const trav_bfs_opts *opts,
+             int32_t *levels, int32_t mem);
+
+/* SSSP distances from each of n sources: dist[q*V + v].  Replaces
+ * SingleSourceShortestPaths::gpu_bellman_ford (algorithm/sssp/sssp.hpp:219-277)
+ * and bellman_ford_wrapper (algorithm/sssp/gpu/bellman_ford.cu:103-144). */
+int trav_sssp(trav_graph *g, const int32_t *sources, int32_t n, const trav_sssp_opts *opts,
+              float *dist, int32_t mem);
+
+/* Statistics of the last query (of the last source of a batch). */
+int trav_last_stats(trav_graph *g, trav_query_stats *out);
+
+/* Device time (ms, CUDA events on the launching stream) of each traversal
+ * launch of the last batch; *n receives the batch size. */
+int trav_last_batch_ms(trav_graph *g, float *ms, int32_t cap, int32_t *n);
+
+/* Run this handle's queries on the caller's CUDA stream (a cudaStream_t;
+ * NULL restores the handle's own stream).  Calls still return after their
+ * work has finished. */
+int trav_graph_set_stream(trav_graph *g, void *stream);
+
+/* Per-step trace of the last BFS query: dirs[s] (0 top-down, 1 bottom-up) and
+ * frontier[s] (vertices on the frontier of step s), up to cap entries.
+ * *nsteps receives the step count. */
+int trav_last_bfs_trace(trav_graph *g, uint8_t *dirs, int64_t *frontier, int32_t cap, int32_t *nsteps);
+
+/* ------------------------------------- reference-shaped entry points (EL) */
+
+/* init_kernel / init_distances_wrapper<float> (algorithm/sssp/gpu/
+ * bellman_ford.cu:10-56): d[i] = FLT_MAX, d[source] = 0 on device memory. */
+int trav_init_distances_f32(float *d, int32_t vertices, int32_t source);
+
+/* bellman_ford_wrapper<float> (algorithm/sssp/gpu/bellman_ford.cu:103-144):
+ * device edge-list arrays, relaxes the caller's device distance array d to
+ * its fixpoint (from whatever d holds, as the reference does). */
+int trav_bellman_ford_el_f32(const int32_t *src, const int32_t *dst, const float *w, int32_t vertices,
+                             int64_t edges, int32_t source, float *d);
+
+/* bfs_wrapper (algorithm/bfs/gpu/bfs.cu:43-81): device edge-list arrays,
+ * writes visited[v] = 1 / 0 (C++ bool layout) to device memory. */
+int trav_bfs_el(const int32_t *src, const int32_t *dst, int32_t vertices, int64_t edges, uint8_t *visited,
+                int32_t source);
+
+/* -------------------------------------------------- graph files (host only) */
+
+/* Read an edge-list binary file in the reference format
+ * (include/storage/graph_storage_API.hpp:114-160): bool directed, int32 V,
+ * int64 E, then E records {int32 src, int32 dst, float w}.  Call with
+ * src == NULL to get V, E and directed only.  With unweighted != 0 the records
+ * are {int32 src, int32 dst} (generator.cpp:51-72) and w is filled with 1.0. */
+int trav_el_file_read(const char *path, int32_t unweighted, int32_t *vertices, int64_t *edges,
+                      int32_t *directed, int32_t *src, int32_t *dst, float *w);
+
+/* Write the same format (include/storage/graph_storage_API.hpp:39-65). */
+int trav_el_file_write(const char *path, int32_t directed, int32_t vertices, int64_t edges,
+                       const int32_t *src, const int32_t *dst, const float *w);
+
+/* ------------------------------------------------------- learned schedule */
+
+/* Install the parameters of a schedule MLP on a handle (copied to the
+ * device).  kind 0 = BFS direction (2 outputs: top-down, bottom-up);
+ * kind 1 = SSSP bucket width (4 outputs: delta x 1, 2, 4, 8).  count must be
+ * trav_mlp_param_count(kind).  Layout: [W1 (32x10) | b1 (32) | W2 (32x32) |
+ * b2 (32) | W3 (Ox32) | b3 (O)], row-major, tanh hidden units.  New; the
+ * reference has no learned schedule. */
+int trav_mlp_set(trav_graph *g, int32_t kind, const float *params, int32_t count);
+int32_t trav_mlp_param_count(int32_t kind);
+
+/* ------------------------------------------------------------------- misc */
+
+const char *trav_last_error(void);
+const char *trav_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TRAV_H */

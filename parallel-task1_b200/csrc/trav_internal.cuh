@@ -1,0 +1,146 @@
+// Internal declarations shared by the traversal library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/trav.h"
+
+namespace trav {
+
+constexpr int kBlock = 256;       // threads per CTA of the persistent kernels
+constexpr int kWarps = kBlock / 32;
+constexpr int kChunk = 512;       // edges per chunk item of a high-degree row
+constexpr int kBigDegree = 512;   // rows longer than this are split into chunks
+constexpr int kMaxTrace = 4096;   // steps recorded per query
+constexpr int kSlots = 4;         // ring of per-phase counter slots
+
+// Device status codes written to Ctl::err.
+constexpr int kErrTimeout = 1;    // a bounded grid-barrier wait gave up
+constexpr int kErrBudget = 2;     // the step budget of a query ran out
+
+// Counters produced by one phase; read by every CTA after the next barrier.
+struct Slot {
+    unsigned int q_add;           // entries appended to the next queue
+    unsigned int far_add;         // entries appended to the far pile
+    unsigned int chunk_add;       // chunk items appended
+    int min_far_bits;             // min distance bits pushed to the far pile
+    unsigned long long mf;        // out-degree sum of newly reached vertices
+    unsigned long long pad;
+};
+
+// Control block of one persistent launch (zeroed by the host before launch).
+struct Ctl {
+    unsigned int bar_count;
+    unsigned int bar_gen;
+    int err;
+    int err_phase;
+    Slot slot[kSlots];
+    // written by CTA 0 as the query runs
+    int steps;
+    int buckets;
+    int bottom_up_steps;
+    int next_id;                  // first unused stamp id after the query
+    unsigned char dirs[kMaxTrace];
+    unsigned int frontier[kMaxTrace];
+};
+
+// Device graph: int32 CSR over relabelled ids + transposed CSR.
+struct DevGraph {
+    int32_t V = 0;
+    int64_t E = 0;
+    int32_t max_out_degree = 0;
+    int32_t *out_off = nullptr;   // V+1
+    int32_t *out_adj = nullptr;   // E
+    float *out_w = nullptr;       // E
+    int32_t *in_off = nullptr;    // V+1
+    int32_t *in_adj = nullptr;    // E
+    int32_t *new_of_old = nullptr;  // V
+    int32_t *old_of_new = nullptr;  // V
+};
+
+// Per-handle traversal workspace (scratch memory of the persistent kernels).
+struct Workspace {
+    int32_t V = 0;
+    int64_t chunk_cap = 0;
+    unsigned int *value = nullptr;     // V: BFS level (int32) or SSSP distance bits
+    unsigned int *visited = nullptr;   // W words
+    unsigned int *front[2] = {nullptr, nullptr};  // W words each
+    int32_t *queue[2] = {nullptr, nullptr};       // V each
+    int32_t *far[2] = {nullptr, nullptr};         // V each
+    int32_t *stamp_near = nullptr;     // V
+    int32_t *stamp_far = nullptr;      // V
+    int2 *chunks = nullptr;            // chunk_cap
+    Ctl *ctl = nullptr;                // ctl_cap control blocks: one per query of a batch
+    int ctl_cap = 0;
+    int *id_base = nullptr;            // device: first unused stamp id (continues across queries)
+};
+
+// Arguments of the persistent kernels (passed by value).
+struct TravArgs {
+    // graph (read-only for the launch)
+    const int32_t *__restrict__ out_off;
+    const int32_t *__restrict__ out_adj;
+    const float *__restrict__ out_w;
+    const int32_t *__restrict__ in_off;
+    const int32_t *__restrict__ in_adj;
+    const int32_t *__restrict__ new_of_old;
+    int32_t V;
+    int32_t W;        // bitmap words
+    int64_t E;
+    // workspace
+    unsigned int *value;
+    unsigned int *visited;
+    unsigned int *front0, *front1;
+    int32_t *q0, *q1;
+    int32_t *far0, *far1;
+    int32_t *stamp_near, *stamp_far;
+    int2 *chunks;
+    Ctl *ctl;
+    // query
+    int32_t source;        // new id; -1 = start from the distances in `value`
+    int32_t max_steps;
+    int *id_base;          // device: first stamp id this query may use; updated at the end
+    // BFS options
+    float alpha, beta;
+    int32_t force_dir;
+    // SSSP options
+    float delta;           // +inf = Bellman-Ford
+    // output (original ids); nullptr = leave results in `value`
+    void *out;
+    int32_t out_kind;      // 0 = int32 levels, 1 = float distances, 2 = uint8 reached flags
+    // learned schedule (nullptr = plain)
+    const float *mlp;
+    unsigned long long timeout_ns;
+};
+
+// ---- host-side helpers (capi.cu) ----
+void set_error(const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+// ingest.cu
+int build_graph_device(int32_t V, int64_t E, const int32_t *d_src, const int32_t *d_dst, const float *d_w,
+                       cudaStream_t st, DevGraph *out);
+void free_graph(DevGraph *g);
+int rmat_device(int scale, int avg, int a, int b, int c, int d, uint32_t seed, int drop_loops,
+                int32_t *d_src, int32_t *d_dst, float *d_w, int64_t *E_out, cudaStream_t st);
+int validate_edges(int32_t V, int64_t E, const int32_t *d_src, const int32_t *d_dst, const float *d_w,
+                   cudaStream_t st);
+
+// traverse.cu
+int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_t st);
+void workspace_free(Workspace *ws);
+// Enqueue one query on st using control block ws->ctl[q] (no host sync).
+// ev0/ev1 (optional) are recorded around the launch.
+int launch_bfs(const DevGraph &g, Workspace *ws, int q, int32_t source_new, const trav_bfs_opts &o,
+               const float *mlp, void *out, int out_kind, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1);
+int launch_sssp(const DevGraph &g, Workspace *ws, int q, int32_t source_new, float delta, const float *mlp,
+                void *out, int out_kind, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1);
+// After the stream finished: turn the device status of queries [0, n) into a return code.
+int check_queries(Workspace *ws, int n, const char *what);
+int query_bytes(const DevGraph &g, Workspace *ws, int q, int kind, int64_t *bytes, int64_t *reached,
+                int64_t *reached_edges, cudaStream_t st);
+int persistent_grid_size(int kind);
+
+}  // namespace trav

@@ -1,0 +1,300 @@
+"""Python binding of the B200 traversal library (ctypes over include/trav.h).
+
+Mirrors the reference's operator surface for the traversal path:
+
+* ``Graph`` -- a device graph built from an edge list (``from_edges``), a
+  reference-format edge-list file (``load_edges_list``) or the seeded device
+  RMAT generator (``rmat``, restating ``GraphGenerationAPI::R_MAT_parallel``,
+  include/test/generation/graph_generation_API.hpp:403-484).
+* ``Graph.bfs`` / ``Graph.sssp`` -- ``BFS::gpu_bfs`` (algorithm/bfs/bfs.hpp:
+  212-254) and ``SingleSourceShortestPaths::gpu_bellman_ford`` (algorithm/sssp/
+  sssp.hpp:219-277), batched over sources, returning levels / fp32 distances in
+  the caller's vertex ids.
+* ``init_distances``, ``bellman_ford_wrapper``, ``bfs_wrapper`` -- the
+  reference's device-pointer wrappers (algorithm/sssp/gpu/bellman_ford.cu:
+  38-144, algorithm/bfs/gpu/bfs.cu:43-81).
+
+Errors raise ``TravError`` carrying the library's status code and message;
+there is no CPU fallback: without the compiled library or a GPU the calls fail.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG, "libtrav_b200.so")
+
+TRAV_OK = 0
+TRAV_ERR_BAD_ARG = -1
+TRAV_ERR_OOM = -2
+TRAV_ERR_OVERFLOW_INT32 = -3
+TRAV_ERR_TIMEOUT = -4
+TRAV_ERR_CUDA = -5
+TRAV_ERR_NO_DEVICE = -6
+TRAV_ERR_IO = -7
+MEM_HOST, MEM_DEVICE = 0, 1
+SCHEDULE_PLAIN, SCHEDULE_LEARNED = 0, 1
+FLT_MAX = np.float32(np.finfo(np.float32).max)
+
+# Every symbol include/trav.h declares (checked by the CPU test suite).
+EXPORTS = [
+    "trav_graph_from_edges", "trav_graph_rmat", "trav_graph_free", "trav_graph_info", "trav_graph_export",
+    "trav_bfs", "trav_sssp", "trav_last_stats", "trav_last_bfs_trace", "trav_init_distances_f32",
+    "trav_bellman_ford_el_f32", "trav_bfs_el", "trav_el_file_read", "trav_el_file_write", "trav_mlp_set",
+    "trav_mlp_param_count", "trav_last_error", "trav_version", "trav_last_batch_ms", "trav_graph_set_stream",
+]
+
+
+class TravError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"trav error {code}: {msg}")
+        self.code = code
+
+
+class BfsOpts(C.Structure):
+    _fields_ = [("schedule", C.c_int32), ("alpha", C.c_float), ("beta", C.c_float), ("force_direction", C.c_int32)]
+
+
+class SsspOpts(C.Structure):
+    _fields_ = [("schedule", C.c_int32), ("delta", C.c_float)]
+
+
+class QueryStats(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("steps", C.c_int32), ("buckets", C.c_int32), ("bottom_up_steps", C.c_int32),
+                ("reached", C.c_int64), ("reached_edges", C.c_int64), ("algorithmic_bytes", C.c_int64),
+                ("kernel_ms", C.c_float)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python parallel-task1_b200/build.py`")
+        L = C.CDLL(LIB_PATH)
+        vp, i32, i64, f32 = C.c_void_p, C.c_int32, C.c_int64, C.c_float
+        L.trav_last_error.restype = C.c_char_p
+        L.trav_version.restype = C.c_char_p
+        L.trav_graph_from_edges.argtypes = [i32, i64, vp, vp, vp, i32, C.POINTER(vp)]
+        L.trav_graph_rmat.argtypes = [i32] * 6 + [C.c_uint32, i32, vp, vp, vp, C.POINTER(i64), C.POINTER(vp)]
+        L.trav_graph_free.argtypes = [vp]
+        L.trav_graph_info.argtypes = [vp, C.POINTER(i32), C.POINTER(i64), C.POINTER(i32)]
+        L.trav_graph_export.argtypes = [vp] * 8
+        L.trav_bfs.argtypes = [vp, vp, i32, C.POINTER(BfsOpts), vp, i32]
+        L.trav_sssp.argtypes = [vp, vp, i32, C.POINTER(SsspOpts), vp, i32]
+        L.trav_last_stats.argtypes = [vp, C.POINTER(QueryStats)]
+        L.trav_last_bfs_trace.argtypes = [vp, vp, vp, i32, C.POINTER(i32)]
+        L.trav_init_distances_f32.argtypes = [vp, i32, i32]
+        L.trav_bellman_ford_el_f32.argtypes = [vp, vp, vp, i32, i64, i32, vp]
+        L.trav_bfs_el.argtypes = [vp, vp, i32, i64, vp, i32]
+        L.trav_el_file_read.argtypes = [C.c_char_p, i32, C.POINTER(i32), C.POINTER(i64), C.POINTER(i32), vp, vp, vp]
+        L.trav_el_file_write.argtypes = [C.c_char_p, i32, i32, i64, vp, vp, vp]
+        L.trav_mlp_set.argtypes = [vp, i32, vp, i32]
+        L.trav_mlp_param_count.argtypes = [i32]
+        L.trav_mlp_param_count.restype = i32
+        L.trav_last_batch_ms.argtypes = [vp, vp, i32, C.POINTER(i32)]
+        L.trav_graph_set_stream.argtypes = [vp, vp]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != TRAV_OK:
+        raise TravError(rc, lib().trav_last_error().decode())
+
+
+def _ptr(a):
+    """Data pointer of a numpy array or a torch tensor (host or CUDA)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+def _is_cuda(a) -> bool:
+    return hasattr(a, "is_cuda") and bool(a.is_cuda)
+
+
+@dataclass
+class Stats:
+    kind: str
+    steps: int
+    buckets: int
+    bottom_up_steps: int
+    reached: int
+    reached_edges: int
+    algorithmic_bytes: int
+    kernel_ms: float
+
+
+class Graph:
+    """A graph resident on the current CUDA device."""
+
+    def __init__(self, handle):
+        self._h = C.c_void_p(handle)
+        V, E, md = C.c_int32(), C.c_int64(), C.c_int32()
+        _check(lib().trav_graph_info(self._h, C.byref(V), C.byref(E), C.byref(md)))
+        self.V, self.E, self.max_out_degree = V.value, E.value, md.value
+
+    # -------------------------------------------------------------- builders
+    @classmethod
+    def from_edges(cls, V: int, src, dst, w=None):
+        """Edge list as numpy arrays (host) or CUDA tensors (device)."""
+        mem = MEM_DEVICE if _is_cuda(src) else MEM_HOST
+        if mem == MEM_HOST:
+            src = np.ascontiguousarray(src, np.int32)
+            dst = np.ascontiguousarray(dst, np.int32)
+            w = None if w is None else np.ascontiguousarray(w, np.float32)
+        h = C.c_void_p()
+        _check(lib().trav_graph_from_edges(V, len(src), _ptr(src), _ptr(dst), _ptr(w), mem, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def rmat(cls, scale: int, avg: int, abcd=(57, 19, 19, 5), seed: int = 1, drop_self_loops: bool = True,
+             edges_out=None):
+        """Seeded device RMAT; edges_out=(src, dst, w) CUDA tensors of V*avg entries receive the edge list."""
+        h = C.c_void_p()
+        E = C.c_int64()
+        s, d, w = edges_out if edges_out is not None else (None, None, None)
+        _check(lib().trav_graph_rmat(scale, avg, *abcd, seed & 0xFFFFFFFF, int(drop_self_loops), _ptr(s), _ptr(d),
+                                     _ptr(w), C.byref(E), C.byref(h)))
+        g = cls(h.value)
+        g.generated_edges = E.value
+        return g
+
+    @classmethod
+    def load_edges_list(cls, path: str, unweighted: bool = False):
+        src, dst, w, V, _directed = read_edges_list(path, unweighted)
+        return cls.from_edges(V, src, dst, w)
+
+    def free(self):
+        if self._h is not None and self._h.value:
+            lib().trav_graph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    # --------------------------------------------------------------- queries
+    def bfs(self, sources, out=None, schedule=SCHEDULE_PLAIN, alpha=15.0, beta=18.0, force_direction=-1):
+        """Levels [n, V] (int32, -1 unreachable).  out: numpy (host) or CUDA tensor (device)."""
+        src = np.ascontiguousarray(np.atleast_1d(sources), np.int32)
+        if out is None:
+            out = np.empty((len(src), self.V), np.int32)
+        mem = MEM_DEVICE if _is_cuda(out) else MEM_HOST
+        o = BfsOpts(schedule, alpha, beta, force_direction)
+        _check(lib().trav_bfs(self._h, src.ctypes.data, len(src), C.byref(o), _ptr(out), mem))
+        return out
+
+    def sssp(self, sources, out=None, delta=0.0, schedule=SCHEDULE_PLAIN):
+        """Distances [n, V] (fp32, FLT_MAX unreachable).  delta <= 0 or inf: Bellman-Ford."""
+        src = np.ascontiguousarray(np.atleast_1d(sources), np.int32)
+        if out is None:
+            out = np.empty((len(src), self.V), np.float32)
+        mem = MEM_DEVICE if _is_cuda(out) else MEM_HOST
+        o = SsspOpts(schedule, delta)
+        _check(lib().trav_sssp(self._h, src.ctypes.data, len(src), C.byref(o), _ptr(out), mem))
+        return out
+
+    def last_stats(self) -> Stats:
+        s = QueryStats()
+        _check(lib().trav_last_stats(self._h, C.byref(s)))
+        return Stats("bfs" if s.kind == 0 else "sssp", s.steps, s.buckets, s.bottom_up_steps, s.reached,
+                     s.reached_edges, s.algorithmic_bytes, s.kernel_ms)
+
+    def last_bfs_trace(self):
+        cap = 4096
+        dirs = np.zeros(cap, np.uint8)
+        fr = np.zeros(cap, np.int64)
+        n = C.c_int32()
+        _check(lib().trav_last_bfs_trace(self._h, dirs.ctypes.data, fr.ctypes.data, cap, C.byref(n)))
+        k = min(n.value, cap)
+        return dirs[:k].copy(), fr[:k].copy()
+
+    def last_batch_ms(self):
+        """Device time (ms) of each launch of the last batch."""
+        n = C.c_int32()
+        _check(lib().trav_last_batch_ms(self._h, None, 0, C.byref(n)))
+        ms = np.zeros(max(n.value, 1), np.float32)
+        _check(lib().trav_last_batch_ms(self._h, ms.ctypes.data, n.value, C.byref(n)))
+        return ms[: n.value]
+
+    def set_stream(self, stream):
+        """Run queries on a CUDA stream (int handle or torch.cuda.Stream); None = the handle's own."""
+        h = getattr(stream, "cuda_stream", stream)
+        _check(lib().trav_graph_set_stream(self._h, C.c_void_p(h) if h else None))
+
+    def set_mlp(self, kind: int, params):
+        p = np.ascontiguousarray(params, np.float32)
+        _check(lib().trav_mlp_set(self._h, kind, p.ctypes.data, len(p)))
+
+    def out_degrees(self):
+        """Out-degree of every vertex in the caller's ids."""
+        n2o = np.empty(self.V, np.int32)
+        oo = np.empty(self.V + 1, np.int32)
+        _check(lib().trav_graph_export(self._h, n2o.ctypes.data, None, oo.ctypes.data, None, None, None, None))
+        return np.diff(oo)[n2o]
+
+    def export_layout(self):
+        V, E = self.V, self.E
+        n2o = np.empty(V, np.int32)
+        o2n = np.empty(V, np.int32)
+        oo = np.empty(V + 1, np.int32)
+        oa = np.empty(max(E, 1), np.int32)
+        ow = np.empty(max(E, 1), np.float32)
+        io = np.empty(V + 1, np.int32)
+        ia = np.empty(max(E, 1), np.int32)
+        _check(lib().trav_graph_export(self._h, *(x.ctypes.data for x in (n2o, o2n, oo, oa, ow, io, ia))))
+        return dict(new_of_old=n2o, old_of_new=o2n, out_off=oo, out_adj=oa[:E], out_w=ow[:E], in_off=io,
+                    in_adj=ia[:E])
+
+
+def mlp_param_count(kind: int) -> int:
+    return int(lib().trav_mlp_param_count(kind))
+
+
+# ----------------------------------------------- reference-shaped wrappers
+def init_distances(d, V: int, source: int):
+    """init_distances_wrapper<float> on a CUDA float tensor."""
+    _check(lib().trav_init_distances_f32(_ptr(d), V, source))
+
+
+def bellman_ford_wrapper(src, dst, w, V: int, E: int, source: int, d):
+    """bellman_ford_wrapper<float> on CUDA tensors; relaxes d in place."""
+    _check(lib().trav_bellman_ford_el_f32(_ptr(src), _ptr(dst), _ptr(w), V, E, source, _ptr(d)))
+
+
+def bfs_wrapper(src, dst, V: int, E: int, visited, source: int):
+    """bfs_wrapper on CUDA tensors; visited is a uint8/bool CUDA tensor of V entries."""
+    _check(lib().trav_bfs_el(_ptr(src), _ptr(dst), V, E, _ptr(visited), source))
+
+
+# --------------------------------------------------------------- files
+def read_edges_list(path: str, unweighted: bool = False):
+    V, E, D = C.c_int32(), C.c_int64(), C.c_int32()
+    p = path.encode()
+    _check(lib().trav_el_file_read(p, int(unweighted), C.byref(V), C.byref(E), C.byref(D), None, None, None))
+    src = np.empty(E.value, np.int32)
+    dst = np.empty(E.value, np.int32)
+    w = np.empty(E.value, np.float32)
+    _check(lib().trav_el_file_read(p, int(unweighted), C.byref(V), C.byref(E), C.byref(D), src.ctypes.data,
+                                   dst.ctypes.data, w.ctypes.data))
+    return src, dst, w, V.value, bool(D.value)
+
+
+def write_edges_list(path: str, V: int, src, dst, w, directed: bool = True):
+    src = np.ascontiguousarray(src, np.int32)
+    dst = np.ascontiguousarray(dst, np.int32)
+    w = np.ascontiguousarray(w, np.float32)
+    _check(lib().trav_el_file_write(path.encode(), int(directed), V, len(src), src.ctypes.data, dst.ctypes.data,
+                                    w.ctypes.data))
