@@ -548,6 +548,10 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
             steps++;
             if (gtid == 0 && steps - 1 < kMaxTrace) ctl->frontier[steps - 1] = (unsigned)qlen;
         } else if (far_len > 0) {
+            if (buckets >= a.max_steps) {
+                if (gtid == 0) atomicCAS(&ctl->err, 0, kErrBudget);
+                return;
+            }
             // open the next bucket (skipping empty ones): bound = max(old, min far) + width
             if (threadIdx.x < 32) {
                 float d = a.delta;
