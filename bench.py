@@ -63,9 +63,32 @@ def workload_name(a):
 
 
 def pick_sources(deg, n, seed):
+    """n distinct seeded sources among vertices of nonzero out-degree (sorted)."""
     rng = np.random.default_rng(seed)
     cand = np.flatnonzero(deg > 0)
     return np.sort(rng.choice(cand, size=min(n, len(cand)), replace=False)).astype(np.int32)
+
+
+def rank_sources(deg, n, seed, rank):
+    """Replica r of a weak-scaling run traverses its own seeded source set."""
+    return pick_sources(deg, n, seed + rank)
+
+
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """Max of a per-rank time over the process group (the slowest replica sets the job time)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_gteps(traversals_per_rank: int, edges: int, world: int, seconds_max: float) -> float:
+    """Whole-job GTEPS: every rank's traversals x E over the max-over-ranks time."""
+    return world * traversals_per_rank * edges / seconds_max / 1e9
 
 
 # --------------------------------------------------------------- clocks
@@ -247,7 +270,7 @@ def run_ours(a):
     ingest_s = time.perf_counter() - t0
     V, E = g.V, g.E
     deg = g.out_degrees()
-    sources = pick_sources(deg, a.sources, a.seed + rank)
+    sources = rank_sources(deg, a.sources, a.seed, rank)
     n = len(sources)
 
     stream = torch.cuda.current_stream()
@@ -290,13 +313,9 @@ def run_ours(a):
     clk = clocks.stop()
     if world > 1:
         dist.barrier()
-    ms_total = e0.elapsed_time(e1)
-    t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(e0.elapsed_time(e1), world, dev)
     traversals = 2 * n * a.steps
-    value = world * traversals * E / (ms_max / 1e3) / 1e9
+    value = job_gteps(traversals, E, world, ms_max / 1e3)
 
     # e2e through the public API with pinned host buffers: per step, H2D of the source ids (inside the call)
     # and D2H of every level / distance array, timed on the host clock around the synchronous calls
@@ -319,10 +338,7 @@ def run_ours(a):
     for _ in range(a.steps):
         e2e_step()
     h1 = time.perf_counter()
-    e2e_s = torch.tensor([h1 - h0], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
-    e2e_value = world * traversals * E / float(e2e_s.item()) / 1e9
+    e2e_value = job_gteps(traversals, E, world, max_over_ranks(h1 - h0, world, dev))
 
     # parity spot check of the timed outputs against the host-path outputs (same kernels, same inputs)
     assert np.array_equal(lv_dev.cpu().numpy(), lvn) and np.array_equal(di_dev.cpu().numpy().view(np.uint32),
