@@ -159,6 +159,34 @@ int trav_bellman_ford_el_f32(const int32_t *src, const int32_t *dst, const float
 int trav_bfs_el(const int32_t *src, const int32_t *dst, int32_t vertices, int64_t edges, uint8_t *visited,
                 int32_t source);
 
+/* ------------------------------------------------- allocation-free BFS */
+
+/* BFS levels (top-down) over a CSR the caller already holds in device
+ * memory, without allocating anything.  This entry point has no counterpart
+ * in the reference.
+ *
+ * It is for callers that cannot call cudaMalloc: a process whose device
+ * memory is owned by another allocator (for example a framework's caching
+ * pool that has reserved the free memory), or a latency-critical service that
+ * cannot accept the device-wide synchronisation cudaMalloc / cudaFree imply.
+ * Every other entry point here allocates its workspace; this one takes all
+ * of its scratch (levels, bitmap, queues, control block) from one static
+ * 8 MiB device array that every GPU which loads the library holds until the
+ * process exits.  Limits: 1 <= vertices <= 262144, 0 <= edges <= 16777216;
+ * larger graphs are rejected with TRAV_ERR_BAD_ARG (use trav_bfs).
+ *
+ * row_offsets (V+1 int32), adj (E int32, ids in [0, V)) and levels (V int32,
+ * written: hop level or -1) are device pointers in the caller's vertex ids;
+ * the CSR is checked before use.  Runs on `stream` (a cudaStream_t; NULL =
+ * the legacy default stream) and returns after the work has finished.
+ * The first call on a device looks up the device address of the static array
+ * (cudaGetSymbolAddress) once for that device; make that first call before
+ * any stream capture begins.  All calls share the one array and leave their
+ * contents in it: calls that overlap on the GPU (from two host threads or two
+ * streams) race and must be serialised by the caller. */
+int trav_bfs_csr_noalloc(const int32_t *row_offsets, const int32_t *adj, int32_t vertices, int64_t edges,
+                         int32_t source, int32_t *levels, void *stream);
+
 /* -------------------------------------------------- graph files (host only) */
 
 /* Read an edge-list binary file in the reference format

@@ -16,6 +16,8 @@
 #include <cfloat>
 #include <climits>
 #include <cmath>
+#include <cstddef>
+#include <mutex>
 
 #include "trav_internal.cuh"
 #include "mlp_device.cuh"
@@ -880,4 +882,183 @@ int query_bytes(const DevGraph &g, Workspace *ws, int q, int kind, int64_t *byte
     return TRAV_OK;
 }
 
+// ------------------------------------------------ allocation-free BFS entry
+// For callers that must not allocate device memory: a process whose device
+// memory is already owned by another allocator (a framework's caching pool
+// that reserved the free memory), or a latency-critical service where the
+// device-wide synchronisation of cudaMalloc / cudaFree is not acceptable.
+// Those callers hold their graph as a CSR in device memory already; this
+// entry point runs the top-down persistent BFS directly on it, taking every
+// byte of scratch (levels, visited bitmap, two frontier queues, chunk items,
+// the control block) from one statically sized device array of this library.
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;   // 8 MiB on every device that loads the library
+constexpr int32_t kNoAllocMaxVertices = 1 << 18;            // 262,144
+constexpr int64_t kNoAllocMaxEdges = int64_t(1) << 24;      // 16,777,216
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+void *g_noalloc_base[kNoAllocMaxDevices];  // device address of g_noalloc_scratch, per device
+std::mutex g_noalloc_mu;
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// The caller's CSR must be well formed before the kernel trusts it.
+__global__ void noalloc_validate_csr(const int32_t *__restrict__ off, const int32_t *__restrict__ adj, int32_t V,
+                                     int64_t E, int *bad)
+{
+    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (int64_t)gridDim.x * blockDim.x;
+    int flag = 0;
+    for (int64_t v = gtid; v <= V; v += nth) {
+        int o = off[v];
+        if (o < 0 || o > E || (v == 0 && o != 0) || (v == V && o != E) || (v > 0 && off[v - 1] > o)) flag = 1;
+    }
+    for (int64_t e = gtid; e < E; e += nth) {
+        int t = adj[e];
+        if (t < 0 || t >= V) flag = 1;
+    }
+    if (flag) atomicOr(bad, 1);
+}
+
+// Top-down-only BFS over the caller's CSR (vertex ids as given, no relabel),
+// the same phases as bfs_persistent's top-down step.
+__global__ void __launch_bounds__(kBlock) bfs_csr_noalloc_kernel(TravArgs a, int32_t *levels)
+{
+    __shared__ TileShared ts;
+    Ctl *ctl = a.ctl;
+    const int gtid = blockIdx.x * kBlock + threadIdx.x, nth = gridDim.x * kBlock;
+    const int s = a.source;
+    int ph = 0;
+    for (int v = gtid; v < a.V; v += nth) reinterpret_cast<int *>(a.value)[v] = v == s ? 0 : -1;
+    for (int w = gtid; w < a.W; w += nth) a.visited[w] = w == (s >> 5) ? 1u << (s & 31) : 0u;
+    if (gtid == 0) a.q0[0] = s;
+    if (!grid_sync(ctl, a.timeout_ns, ph)) return;
+    ph++;
+    unsigned long long qlen = 1;
+    int L = 0, cur = 0;
+    while (qlen > 0) {
+        if (L >= a.max_steps) {
+            if (gtid == 0) atomicCAS(&ctl->err, 0, kErrBudget);
+            return;
+        }
+        const int32_t *q = cur ? a.q1 : a.q0;
+        int32_t *qn = cur ? a.q0 : a.q1;
+        clear_ahead(ctl, ph);
+        BfsTopDown vis{&a, L + 1, qn, 0u, &ctl->slot[ph % kSlots]};
+        expand_tiles(a, q, (unsigned)qlen, vis, ts, &ctl->slot[ph % kSlots]);
+        if (!grid_sync(ctl, a.timeout_ns, ph)) return;
+        SlotView s0 = read_slot(ctl, ph);
+        ph++;
+        clear_ahead(ctl, ph);
+        vis.qbase = s0.q_add;
+        vis.slot = &ctl->slot[ph % kSlots];
+        expand_chunks(a, s0.chunk_add, vis);
+        if (!grid_sync(ctl, a.timeout_ns, ph)) return;
+        SlotView s1 = read_slot(ctl, ph);
+        ph++;
+        qlen = (unsigned long long)s0.q_add + s1.q_add;
+        L++;
+        cur ^= 1;
+    }
+    if (gtid == 0) ctl->steps = L;
+    for (int v = gtid; v < a.V; v += nth) levels[v] = (int32_t)__ldcg(&a.value[v]);
+}
+
+}  // namespace
+
 }  // namespace trav
+
+using namespace trav;
+
+// Declared in include/trav.h.  No cudaMalloc, cudaFree or other allocating
+// call is made here: scratch comes from g_noalloc_scratch, whose device
+// address is looked up once per device (on that device's first call).
+extern "C" int trav_bfs_csr_noalloc(const int32_t *row_offsets, const int32_t *adj, int32_t vertices, int64_t edges,
+                                    int32_t source, int32_t *levels, void *stream)
+{
+    if (!row_offsets || !levels || (edges > 0 && !adj)) {
+        set_error("trav_bfs_csr_noalloc: row_offsets, adj and levels must be device arrays");
+        return TRAV_ERR_BAD_ARG;
+    }
+    if (vertices < 1 || vertices > kNoAllocMaxVertices || edges < 0 || edges > kNoAllocMaxEdges) {
+        set_error("trav_bfs_csr_noalloc: needs 1 <= vertices <= 262144 and 0 <= edges <= 16777216 (its 8 MiB "
+                  "static scratch); use trav_bfs for larger graphs");
+        return TRAV_ERR_BAD_ARG;
+    }
+    if (source < 0 || source >= vertices) {
+        set_error("trav_bfs_csr_noalloc: source vertex out of range [0, V)");
+        return TRAV_ERR_BAD_ARG;
+    }
+    int dev = 0;
+    TRY_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        set_error("trav_bfs_csr_noalloc: device index beyond the supported 64");
+        return TRAV_ERR_BAD_ARG;
+    }
+    unsigned char *base;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_base[dev]) {
+            void *p = nullptr;
+            TRY_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+            g_noalloc_base[dev] = p;
+        }
+        base = static_cast<unsigned char *>(g_noalloc_base[dev]);
+    }
+    const size_t V = (size_t)vertices, W = (V + 31) / 32;
+    const size_t chunk_cap = V + (size_t)edges / kChunk + 1;
+    size_t at = 0;
+    auto carve = [&](size_t bytes) {
+        unsigned char *p = base + at;
+        at += align256(bytes);
+        return p;
+    };
+    TravArgs a{};
+    a.value = reinterpret_cast<unsigned *>(carve(4 * V));
+    a.visited = reinterpret_cast<unsigned *>(carve(4 * W));
+    a.q0 = reinterpret_cast<int32_t *>(carve(4 * V));
+    a.q1 = reinterpret_cast<int32_t *>(carve(4 * V));
+    a.chunks = reinterpret_cast<int2 *>(carve(sizeof(int2) * chunk_cap));
+    a.ctl = reinterpret_cast<Ctl *>(carve(sizeof(Ctl)));
+    int *bad = reinterpret_cast<int *>(carve(sizeof(int)));
+    if (at > kNoAllocScratchBytes) {  // cannot happen within the limits above
+        set_error("trav_bfs_csr_noalloc: scratch layout exceeds the static array");
+        return TRAV_ERR_BAD_ARG;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int sms = 0, per = 0;
+    TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bfs_csr_noalloc_kernel, kBlock, 0));
+    if (per < 1) return cuda_fail(cudaErrorInvalidConfiguration, "bfs_csr_noalloc_kernel occupancy");
+
+    // every call reuses the array: clear the control block and the flag
+    TRY_CUDA(cudaMemsetAsync(a.ctl, 0, offsetof(Ctl, dirs), st));
+    TRY_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), st));
+    noalloc_validate_csr<<<sms * 4, 256, 0, st>>>(row_offsets, adj, vertices, edges, bad);
+    TRY_CUDA(cudaGetLastError());
+    int hbad = 0;
+    TRY_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TRY_CUDA(cudaStreamSynchronize(st));
+    if (hbad) {
+        set_error("trav_bfs_csr_noalloc: row_offsets must rise from 0 to edges and adj ids must lie in [0, V)");
+        return TRAV_ERR_BAD_ARG;
+    }
+    a.out_off = row_offsets;
+    a.out_adj = adj;
+    a.V = vertices;
+    a.W = (int32_t)W;
+    a.E = edges;
+    a.source = source;
+    a.max_steps = vertices + 1;
+    a.force_dir = 0;
+    a.timeout_ns = 10ull * 1000000000ull;
+    void *params[] = {&a, &levels};
+    TRY_CUDA(cudaLaunchCooperativeKernel((void *)bfs_csr_noalloc_kernel, dim3(sms * per), dim3(kBlock), params, 0, st));
+    TRY_CUDA(cudaStreamSynchronize(st));
+    Ctl h;
+    TRY_CUDA(cudaMemcpy(&h, a.ctl, offsetof(Ctl, slot), cudaMemcpyDeviceToHost));
+    return device_timeout_err(h, "trav_bfs_csr_noalloc");
+}

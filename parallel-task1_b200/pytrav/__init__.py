@@ -46,6 +46,7 @@ EXPORTS = [
     "trav_bfs", "trav_sssp", "trav_last_stats", "trav_last_bfs_trace", "trav_init_distances_f32",
     "trav_bellman_ford_el_f32", "trav_bfs_el", "trav_el_file_read", "trav_el_file_write", "trav_mlp_set",
     "trav_mlp_param_count", "trav_last_error", "trav_version", "trav_last_batch_ms", "trav_graph_set_stream",
+    "trav_bfs_csr_noalloc",
 ]
 
 
@@ -100,6 +101,7 @@ def lib():
         L.trav_mlp_param_count.restype = i32
         L.trav_last_batch_ms.argtypes = [vp, vp, i32, C.POINTER(i32)]
         L.trav_graph_set_stream.argtypes = [vp, vp]
+        L.trav_bfs_csr_noalloc.argtypes = [vp, vp, i32, i64, i32, vp, vp]
         _lib = L
     return _lib
 
@@ -277,6 +279,18 @@ def bellman_ford_wrapper(src, dst, w, V: int, E: int, source: int, d):
 def bfs_wrapper(src, dst, V: int, E: int, visited, source: int):
     """bfs_wrapper on CUDA tensors; visited is a uint8/bool CUDA tensor of V entries."""
     _check(lib().trav_bfs_el(_ptr(src), _ptr(dst), V, E, _ptr(visited), source))
+
+
+def bfs_csr_noalloc(row_offsets, adj, V: int, E: int, source: int, levels, stream=None):
+    """Top-down BFS over a device CSR (CUDA int32 tensors) into `levels`, allocating nothing.
+
+    For callers that cannot allocate device memory (memory owned by another allocator, or paths that cannot
+    take cudaMalloc's synchronisation); scratch comes from the library's static 8 MiB device array, so
+    V <= 262144 and E <= 16777216.  Overlapping calls race on that array.
+    """
+    h = getattr(stream, "cuda_stream", stream)
+    _check(lib().trav_bfs_csr_noalloc(_ptr(row_offsets), _ptr(adj), V, E, source, _ptr(levels),
+                                      C.c_void_p(h) if h else None))
 
 
 # --------------------------------------------------------------- files
