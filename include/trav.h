@@ -76,6 +76,7 @@ typedef struct {
     int64_t reached_edges;   /* out-edges of reached vertices */
     int64_t algorithmic_bytes; /* schedule-independent byte count of the query */
     float kernel_ms;         /* device time of the query's traversal launch */
+    int64_t edges_scanned;   /* out-edges expanded by top-down / relaxation steps (re-expansions included) */
 } trav_query_stats;
 
 /* ------------------------------------------------------------------ graphs */
@@ -141,6 +142,15 @@ int trav_graph_set_stream(trav_graph *g, void *stream);
  * frontier[s] (vertices on the frontier of step s), up to cap entries.
  * *nsteps receives the step count. */
 int trav_last_bfs_trace(trav_graph *g, uint8_t *dirs, int64_t *frontier, int32_t cap, int32_t *nsteps);
+
+/* Phase log of the last query (the last source of a batch): per grid-wide
+ * phase, its kind (0 top-down, 1 bottom-up, 2 frontier-bitmap build,
+ * 3 SSSP relaxation round, 4 SSSP bucket opening), the frontier size it
+ * started from, its end time in microseconds after the query's initialisation
+ * and the cumulative out-edges expanded.  Up to cap entries; *n receives the
+ * phase count.  New; the reference has no equivalent. */
+int trav_last_phase_log(trav_graph *g, uint8_t *kind, int64_t *size, double *end_us, int64_t *edges, int32_t cap,
+                        int32_t *n);
 
 /* ------------------------------------- reference-shaped entry points (EL) */
 

@@ -382,6 +382,7 @@ int trav_last_stats(trav_graph *g, trav_query_stats *out)
     out->buckets = h.buckets;
     out->bottom_up_steps = h.bottom_up_steps;
     out->kernel_ms = g->batch_ms[(size_t)q];
+    out->edges_scanned = (int64_t)h.edges_scanned;
     TRY(query_bytes(g->g, &g->ws, q, g->last_kind, &out->algorithmic_bytes, &out->reached, &out->reached_edges, g->st));
     return TRAV_OK;
 }
@@ -400,6 +401,26 @@ int trav_graph_set_stream(trav_graph *g, void *stream)
     TRY_CUDA(cudaSetDevice(g->device));
     TRY_CUDA(cudaStreamSynchronize(g->st));
     g->st = stream ? static_cast<cudaStream_t>(stream) : g->own_st;
+    return TRAV_OK;
+}
+
+int trav_last_phase_log(trav_graph *g, uint8_t *kind, int64_t *size, double *end_us, int64_t *edges, int32_t cap,
+                        int32_t *n)
+{
+    if (!g || !n) return bad("graph handle and n must not be NULL");
+    if (g->last_n < 1) return bad("no query has run on this handle");
+    TRY_CUDA(cudaSetDevice(g->device));
+    std::unique_ptr<Ctl> h(new Ctl);
+    TRY_CUDA(cudaMemcpy(h.get(), g->ws.ctl + (g->last_n - 1), sizeof(Ctl), cudaMemcpyDeviceToHost));
+    *n = h->nphase;
+    int m = h->nphase < cap ? h->nphase : cap;
+    if (m > kMaxTrace) m = kMaxTrace;
+    for (int i = 0; i < m; i++) {
+        if (kind) kind[i] = h->ph_kind[i];
+        if (size) size[i] = h->ph_size[i];
+        if (end_us) end_us[i] = (double)(long long)(h->ph_end_ns[i] - h->t0_ns) * 1e-3;
+        if (edges) edges[i] = (int64_t)h->ph_scanned[i];
+    }
     return TRAV_OK;
 }
 

@@ -11,8 +11,10 @@ namespace trav {
 
 constexpr int kBlock = 256;       // threads per CTA of the persistent kernels
 constexpr int kWarps = kBlock / 32;
-constexpr int kChunk = 512;       // edges per chunk item of a high-degree row
-constexpr int kBigDegree = 512;   // rows longer than this are split into chunks
+constexpr int kChunk = 512;       // edges per chunk item (two-phase expansion of the allocation-free BFS)
+constexpr int kBigDegree = 512;   // rows longer than this are split into chunks there
+constexpr int kSmallDeg = 32;     // one-phase expansion: rows up to this length go to the CTA-tile queue
+constexpr int kItem = 256;        // one-phase expansion: edges per chunk item of a longer row
 constexpr int kMaxTrace = 4096;   // steps recorded per query
 constexpr int kSlots = 4;         // ring of per-phase counter slots
 
@@ -27,7 +29,8 @@ struct Slot {
     unsigned int chunk_add;       // chunk items appended
     int min_far_bits;             // min distance bits pushed to the far pile
     unsigned long long mf;        // out-degree sum of newly reached vertices
-    unsigned long long pad;
+    unsigned int big_add;         // vertices pushed as chunk items (rows longer than kSmallDeg)
+    unsigned int pad;
 };
 
 // Control block of one persistent launch (zeroed by the host before launch).
@@ -42,8 +45,18 @@ struct Ctl {
     int buckets;
     int bottom_up_steps;
     int next_id;                  // first unused stamp id after the query
-    unsigned char dirs[kMaxTrace];
-    unsigned int frontier[kMaxTrace];
+    unsigned long long edges_scanned;  // out-edges expanded (push-side work, all steps)
+    int nphase;                   // phases logged below
+    unsigned char dirs[kMaxTrace];       // BFS: direction of step s (0 top-down, 1 bottom-up)
+    unsigned int frontier[kMaxTrace];    // BFS: frontier size of step s; SSSP: of expansion s
+    // phase log (CTA 0, after each grid barrier): kind (0 top-down, 1 bottom-up,
+    // 2 bitmap build, 3 relaxation round, 4 bucket opening), frontier size,
+    // %globaltimer at the phase's end and cumulative edges_scanned
+    unsigned char ph_kind[kMaxTrace];
+    unsigned int ph_size[kMaxTrace];
+    unsigned long long ph_end_ns[kMaxTrace];
+    unsigned long long ph_scanned[kMaxTrace];
+    unsigned long long t0_ns;     // %globaltimer after initialisation
 };
 
 // Device graph: int32 CSR over relabelled ids + transposed CSR.
@@ -71,7 +84,7 @@ struct Workspace {
     int32_t *far[2] = {nullptr, nullptr};         // V each
     int32_t *stamp_near = nullptr;     // V
     int32_t *stamp_far = nullptr;      // V
-    int2 *chunks = nullptr;            // chunk_cap
+    int2 *chunks[2] = {nullptr, nullptr};  // chunk_cap items each (current / next frontier)
     Ctl *ctl = nullptr;                // ctl_cap control blocks: one per query of a batch
     int ctl_cap = 0;
     int *id_base = nullptr;            // device: first unused stamp id (continues across queries)
@@ -96,7 +109,8 @@ struct TravArgs {
     int32_t *q0, *q1;
     int32_t *far0, *far1;
     int32_t *stamp_near, *stamp_far;
-    int2 *chunks;
+    int2 *chunks;          // chunk items (two-phase expansion)
+    int2 *chunks0, *chunks1;  // chunk items of the current / next frontier (one-phase expansion)
     Ctl *ctl;
     // query
     int32_t source;        // new id; -1 = start from the distances in `value`

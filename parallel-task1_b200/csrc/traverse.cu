@@ -96,6 +96,7 @@ struct SlotView {
     unsigned q_add, far_add, chunk_add;
     int min_far_bits;  // kFltMaxBits when nothing was pushed
     unsigned long long mf;
+    unsigned big_add;
 };
 
 __device__ __forceinline__ SlotView read_slot(const Ctl *ctl, int ph)
@@ -108,6 +109,7 @@ __device__ __forceinline__ SlotView read_slot(const Ctl *ctl, int ph)
     int neg = s->min_far_bits;  // stored as 0x7fffffff - bits via atomicMax
     v.min_far_bits = neg > 0 ? 0x7fffffff - neg : (int)kFltMaxBits;
     v.mf = s->mf;
+    v.big_add = s->big_add;
     return v;
 }
 
@@ -122,6 +124,22 @@ __device__ __forceinline__ void clear_ahead(Ctl *ctl, int ph)
         s->chunk_add = 0;
         s->min_far_bits = 0;
         s->mf = 0;
+        s->big_add = 0;
+    }
+}
+
+// Phase log entry, written by CTA 0 thread 0 right after a grid barrier.
+__device__ __forceinline__ void log_phase(Ctl *ctl, int kind, unsigned size)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const int i = ctl->nphase;
+        if (i < kMaxTrace) {
+            ctl->ph_kind[i] = (unsigned char)kind;
+            ctl->ph_size[i] = size;
+            ctl->ph_end_ns[i] = globaltimer();
+            ctl->ph_scanned[i] = *(volatile unsigned long long *)&ctl->edges_scanned;
+        }
+        ctl->nphase = i + 1;
     }
 }
 
@@ -174,47 +192,6 @@ struct BfsTopDown {
         }
         warp_append(fresh, v, qn, qbase, &slot->q_add);
         warp_add_u64(deg, &slot->mf);
-    }
-};
-
-struct SsspRelax {
-    const TravArgs *a;
-    float thr;          // bucket upper bound (exclusive)
-    int near_id;        // stamp of the next near queue
-    int far_id;         // stamp of the current far epoch
-    int32_t *qn;
-    unsigned qbase;
-    int32_t *farp;
-    unsigned fbase;
-    Slot *slot;
-
-    __device__ __forceinline__ float begin(int u) const { return __uint_as_float(__ldcg(&a->value[u])); }
-
-    __device__ __forceinline__ void visit(int, float du, int e, bool valid) const
-    {
-        bool imp = false;
-        int v = 0;
-        float nd = 0.0f;
-        if (valid) {
-            v = __ldg(&a->out_adj[e]);
-            nd = __fadd_rn(du, __ldg(&a->out_w[e]));  // one rounded add, as sssp.hpp:56
-            if (nd < __uint_as_float(__ldcg(&a->value[v]))) {
-                int old = atomicMin(reinterpret_cast<int *>(a->value) + v, __float_as_int(nd));
-                imp = nd < __int_as_float(old);
-            }
-        }
-        bool near = false, far = false;
-        if (imp) {
-            if (nd < thr) near = atomicExch(&a->stamp_near[v], near_id) != near_id;
-            else far = atomicExch(&a->stamp_far[v], far_id) != far_id;
-        }
-        warp_append(near, v, qn, qbase, &slot->q_add);
-        if (__any_sync(kFull, far)) {
-            warp_append(far, v, farp, fbase, &slot->far_add);
-            int key = far ? 0x7fffffff - __float_as_int(nd) : 0;
-            key = __reduce_max_sync(kFull, key);
-            if (lane_id() == 0) atomicMax(&slot->min_far_bits, key);
-        }
     }
 };
 
@@ -333,27 +310,379 @@ __device__ void write_back(const TravArgs &a)
     }
 }
 
+// ------------------------------------------------------ one-phase frontier
+// The next frontier is written in two parts while it is discovered: vertices
+// with at most kSmallDeg out-edges go to a queue that the next step expands
+// by CTA tiles; longer rows are cut into kItem-edge items, expanded one warp
+// per item.  Both parts are complete when the step's barrier passes, so a
+// step is one phase and one grid barrier, and the work of long rows is spread
+// over every warp of the grid.
+//
+// Pushes are staged per CTA in shared memory and written out in bulk: one
+// global atomic reserves room for up to a few thousand entries, and the
+// scalar counters (out-degree sums, scanned edges, far minimum) are reduced
+// per CTA per phase.  Without this every warp hit the same few counters and
+// serialised on one L2 slice.  All loops that push are CTA-uniform, so the
+// flush points can use __syncthreads.
+constexpr int kBatch = 4;                      // independent edges per lane per round
+constexpr int kRoundPush = kBlock * kBatch;    // most pushes a CTA makes between two flush points
+constexpr int kFlushQ = 2048, kFlushBig = 256, kFlushFar = 2048;
+
+struct Stage {
+    int q[kFlushQ + kRoundPush];
+    int big[kFlushBig + kRoundPush];
+    int far[kFlushFar + kRoundPush];
+    unsigned nq, nbig, nfar;
+    unsigned base_q, base_far, base_items;
+    unsigned big_total;
+    int far_key;
+    unsigned long long mf, scanned;
+};
+
+// Destination of one phase's pushes.
+struct FrontierOut {
+    int32_t *q;      // short-row queue of the next frontier
+    int2 *chunks;    // chunk items of the next frontier
+    int32_t *farp;   // far pile (SSSP)
+    unsigned fbase;  // far entries already in the pile before this phase
+    Slot *slot;
+};
+
+__device__ __forceinline__ void stage_init(Stage &st)
+{
+    if (threadIdx.x == 0) {
+        st.nq = st.nbig = st.nfar = 0;
+        st.big_total = 0;
+        st.far_key = 0;
+        st.mf = st.scanned = 0;
+    }
+    __syncthreads();
+}
+
+// Warp-collective: lanes with `flag` push vertex v whose row to expand next
+// has `len` edges (tile queue or chunk items by length).
+__device__ __forceinline__ void stage_push(Stage &st, bool flag, int v, unsigned len)
+{
+    const bool big = flag && len > (unsigned)kSmallDeg;
+    const bool small = flag && !big;
+    const unsigned ms = __ballot_sync(kFull, small), mb = __ballot_sync(kFull, big);
+    if (ms) {
+        const unsigned leader = __ffs(ms) - 1;
+        unsigned pos = 0;
+        if (lane_id() == leader) pos = atomicAdd(&st.nq, (unsigned)__popc(ms));
+        pos = __shfl_sync(kFull, pos, leader);
+        if (small) st.q[pos + __popc(ms & lanemask_lt())] = v;
+    }
+    if (mb) {
+        const unsigned leader = __ffs(mb) - 1;
+        unsigned pos = 0;
+        if (lane_id() == leader) {
+            pos = atomicAdd(&st.nbig, (unsigned)__popc(mb));
+            atomicAdd(&st.big_total, (unsigned)__popc(mb));
+        }
+        pos = __shfl_sync(kFull, pos, leader);
+        if (big) st.big[pos + __popc(mb & lanemask_lt())] = v;
+    }
+}
+
+// Warp-collective: lanes with `flag` add v to the far pile; key = 0x7fffffff - distance bits.
+__device__ __forceinline__ void stage_far(Stage &st, bool flag, int v, int key)
+{
+    const unsigned m = __ballot_sync(kFull, flag);
+    if (!m) return;
+    const unsigned leader = __ffs(m) - 1;
+    unsigned pos = 0;
+    if (lane_id() == leader) pos = atomicAdd(&st.nfar, (unsigned)__popc(m));
+    pos = __shfl_sync(kFull, pos, leader);
+    if (flag) st.far[pos + __popc(m & lanemask_lt())] = v;
+    key = __reduce_max_sync(kFull, flag ? key : 0);
+    if (lane_id() == 0) atomicMax(&st.far_key, key);
+}
+
+__device__ __forceinline__ void stage_add_mf(Stage &st, unsigned x)
+{
+    const unsigned s = __reduce_add_sync(kFull, x);
+    if (s && lane_id() == 0) atomicAdd(&st.mf, (unsigned long long)s);
+}
+
+// CTA-collective: write staged entries out when a buffer passed its flush
+// mark (or all of them when `final`, which also publishes the counters).
+// Between two calls a CTA pushes at most kRoundPush entries per buffer.
+__device__ void stage_flush(const TravArgs &a, Stage &st, TileShared &ts, const FrontierOut &o, bool final)
+{
+    __syncthreads();
+    const unsigned nq = st.nq, nbig = st.nbig, nfar = st.nfar;
+    const bool dq = nq > 0 && (final || nq >= (unsigned)kFlushQ);
+    const bool db = nbig > 0 && (final || nbig >= (unsigned)kFlushBig);
+    const bool df = nfar > 0 && (final || nfar >= (unsigned)kFlushFar);
+    if (dq || db || df) {
+        if (threadIdx.x == 0) {
+            if (dq) st.base_q = atomicAdd(&o.slot->q_add, nq);
+            if (df) st.base_far = o.fbase + atomicAdd(&o.slot->far_add, nfar);
+        }
+        if (db) {
+            for (unsigned r = 0; r < nbig; r += kBlock) {
+                const unsigned i = r + threadIdx.x;
+                int v = 0, rb = 0, nch = 0;
+                if (i < nbig) {
+                    v = st.big[i];
+                    rb = __ldg(&a.out_off[v]);
+                    nch = (__ldg(&a.out_off[v + 1]) - rb + kItem - 1) / kItem;
+                }
+                const int pre = block_excl_scan(nch, ts);
+                if (threadIdx.x == 0) st.base_items = atomicAdd(&o.slot->chunk_add, (unsigned)ts.total);
+                __syncthreads();
+                const unsigned base = st.base_items + (unsigned)pre;
+                for (int c = 0; c < nch; c++) o.chunks[base + c] = make_int2(v, rb + c * kItem);
+                __syncthreads();
+            }
+        }
+        __syncthreads();
+        if (dq)
+            for (unsigned i = threadIdx.x; i < nq; i += kBlock) o.q[st.base_q + i] = st.q[i];
+        if (df)
+            for (unsigned i = threadIdx.x; i < nfar; i += kBlock) o.farp[st.base_far + i] = st.far[i];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (dq) st.nq = 0;
+            if (db) st.nbig = 0;
+            if (df) st.nfar = 0;
+        }
+    }
+    if (final && threadIdx.x == 0) {
+        if (st.mf) atomicAdd(&o.slot->mf, st.mf);
+        if (st.scanned) atomicAdd(&a.ctl->edges_scanned, st.scanned);
+        if (st.big_total) atomicAdd(&o.slot->big_add, st.big_total);
+        if (st.far_key) atomicMax(&o.slot->min_far_bits, st.far_key);
+        st.mf = st.scanned = 0;
+        st.big_total = 0;
+        st.far_key = 0;
+    }
+    __syncthreads();
+}
+
+// Expand a frontier in one phase: chunk items (one warp each, kWarps items
+// per CTA iteration), then the short-row queue by CTA tiles (edge-balanced
+// within the tile).  Every lane carries kBatch independent edges per round so
+// their loads and atomics overlap.
+template <class Vis>
+__device__ void expand_frontier(const TravArgs &a, const int32_t *q, unsigned nq, const int2 *chunks, unsigned nch,
+                                const Vis &vis, TileShared &ts, Stage &st, const FrontierOut &o)
+{
+    const int lane = (int)lane_id();
+    const unsigned wic = threadIdx.x >> 5;
+    for (unsigned c0 = blockIdx.x * kWarps; c0 < nch; c0 += gridDim.x * kWarps) {
+        const unsigned c = c0 + wic;
+        int u = 0, start = 0, end = 0;
+        float du = 0.0f;
+        if (c < nch) {
+            const int2 it = __ldcg(&chunks[c]);
+            u = it.x;
+            start = it.y;
+            end = min(start + kItem, __ldg(&a.out_off[u + 1]));
+            du = vis.begin(u);
+            if (lane == 0) atomicAdd(&st.scanned, (unsigned long long)(end - start));
+        }
+        for (int r = 0; r < kItem; r += 32 * kBatch) {  // same trip count in every warp of the CTA
+            int us[kBatch], e[kBatch];
+            float ds[kBatch];
+            bool ok[kBatch];
+#pragma unroll
+            for (int j = 0; j < kBatch; j++) {
+                e[j] = start + r + lane + 32 * j;
+                ok[j] = e[j] < end;
+                us[j] = u;
+                ds[j] = du;
+            }
+            if (__any_sync(kFull, ok[0])) vis.visit_batch(us, ds, e, ok, st);
+            stage_flush(a, st, ts, o, false);
+        }
+    }
+    for (unsigned tile = blockIdx.x * kBlock; tile < nq; tile += gridDim.x * kBlock) {
+        const unsigned i = tile + threadIdx.x;
+        int u = 0, rb = 0, deg = 0;
+        if (i < nq) {
+            u = __ldcg(&q[i]);
+            rb = __ldg(&a.out_off[u]);
+            deg = __ldg(&a.out_off[u + 1]) - rb;
+        }
+        const int pre = block_excl_scan(deg, ts);
+        ts.u[threadIdx.x] = u;
+        ts.rb[threadIdx.x] = rb;
+        ts.pre[threadIdx.x] = pre;
+        ts.du[threadIdx.x] = deg > 0 ? vis.begin(u) : 0.0f;
+        __syncthreads();
+        const int total = ts.total;
+        if (threadIdx.x == 0 && total) atomicAdd(&st.scanned, (unsigned long long)total);
+        const int n = (int)min((unsigned)kBlock, nq - tile);
+        for (int base = 0; base < total; base += kRoundPush) {
+            int us[kBatch], e[kBatch];
+            float ds[kBatch];
+            bool ok[kBatch];
+#pragma unroll
+            for (int j = 0; j < kBatch; j++) {
+                const int k = base + (int)threadIdx.x + kBlock * j;
+                ok[j] = k < total;
+                int lo = 0;
+                if (ok[j]) {
+                    int hi = n;
+                    while (hi - lo > 1) {
+                        const int mid = (lo + hi) >> 1;
+                        if (ts.pre[mid] <= k) lo = mid;
+                        else hi = mid;
+                    }
+                }
+                e[j] = ts.rb[lo] + (k - ts.pre[lo]);
+                us[j] = ts.u[lo];
+                ds[j] = ts.du[lo];
+            }
+            // lanes whose first edge is past the end have none at all
+            if (__any_sync(kFull, ok[0])) vis.visit_batch(us, ds, e, ok, st);
+            stage_flush(a, st, ts, o, false);
+        }
+        __syncthreads();
+    }
+    stage_flush(a, st, ts, o, true);
+}
+
+// Single-source frontier: the source alone (every CTA computes the counts).
+__device__ __forceinline__ void seed_frontier(const TravArgs &a, int s, int32_t *q, int2 *chunks, unsigned &nq,
+                                              unsigned &nch)
+{
+    const int rb = __ldg(&a.out_off[s]);
+    const int deg = __ldg(&a.out_off[s + 1]) - rb;
+    const int gtid = blockIdx.x * kBlock + threadIdx.x, nth = gridDim.x * kBlock;
+    if (deg > kSmallDeg) {
+        nq = 0;
+        nch = (unsigned)((deg + kItem - 1) / kItem);
+        for (int c = gtid; c < (int)nch; c += nth) chunks[c] = make_int2(s, rb + c * kItem);
+    } else {
+        nq = 1;
+        nch = 0;
+        if (gtid == 0) q[0] = s;
+    }
+}
+
+// visit_batch() is called by all 32 lanes of a warp together; ok[j] marks
+// the lanes' edges that exist.  begin() returns the per-vertex value used.
+struct BfsPush {
+    const TravArgs *a;
+    int level_next;
+
+    __device__ __forceinline__ float begin(int) const { return 0.0f; }
+
+    __device__ __forceinline__ void visit_batch(const int (&)[kBatch], const float (&)[kBatch], const int (&e)[kBatch],
+                                                const bool (&ok)[kBatch], Stage &st) const
+    {
+        int v[kBatch];
+        unsigned word[kBatch];
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) v[j] = ok[j] ? __ldg(&a->out_adj[e[j]]) : 0;
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) word[j] = ok[j] ? __ldcg(&a->visited[v[j] >> 5]) : ~0u;
+        bool fresh[kBatch];
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) {
+            const unsigned bit = 1u << (v[j] & 31);
+            fresh[j] = false;
+            if (!(word[j] & bit)) fresh[j] = !(atomicOr(a->visited + (v[j] >> 5), bit) & bit);
+        }
+        unsigned deg[kBatch], dsum = 0;
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) {
+            deg[j] = 0;
+            if (fresh[j]) {
+                reinterpret_cast<int *>(a->value)[v[j]] = level_next;
+                deg[j] = (unsigned)(__ldg(&a->out_off[v[j] + 1]) - __ldg(&a->out_off[v[j]]));
+            }
+            dsum += deg[j];
+        }
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) stage_push(st, fresh[j], v[j], deg[j]);
+        stage_add_mf(st, dsum);
+    }
+};
+
+struct SsspPush {
+    const TravArgs *a;
+    float thr;          // bucket upper bound (exclusive)
+    int near_id;        // stamp of the next near frontier
+    int far_id;         // stamp of the current far epoch
+
+    __device__ __forceinline__ float begin(int u) const { return __uint_as_float(__ldcg(&a->value[u])); }
+
+    __device__ __forceinline__ void visit_batch(const int (&)[kBatch], const float (&du)[kBatch],
+                                                const int (&e)[kBatch], const bool (&ok)[kBatch], Stage &st) const
+    {
+        int v[kBatch];
+        float nd[kBatch];
+        unsigned cur[kBatch];
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) {
+            v[j] = 0;
+            nd[j] = 0.0f;
+            if (ok[j]) {
+                v[j] = __ldg(&a->out_adj[e[j]]);
+                nd[j] = __fadd_rn(du[j], __ldg(&a->out_w[e[j]]));  // one rounded add, as sssp.hpp:56
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) cur[j] = ok[j] ? __ldcg(&a->value[v[j]]) : 0u;
+        bool imp[kBatch];
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) {
+            imp[j] = false;
+            if (ok[j] && nd[j] < __uint_as_float(cur[j])) {
+                const int old = atomicMin(reinterpret_cast<int *>(a->value) + v[j], __float_as_int(nd[j]));
+                imp[j] = nd[j] < __int_as_float(old);
+            }
+        }
+        bool near[kBatch], far[kBatch];
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) {
+            near[j] = far[j] = false;
+            if (imp[j]) {
+                if (nd[j] < thr) near[j] = atomicExch(&a->stamp_near[v[j]], near_id) != near_id;
+                else far[j] = atomicExch(&a->stamp_far[v[j]], far_id) != far_id;
+            }
+        }
+        unsigned deg[kBatch];
+#pragma unroll
+        for (int j = 0; j < kBatch; j++)
+            deg[j] = near[j] ? (unsigned)(__ldg(&a->out_off[v[j] + 1]) - __ldg(&a->out_off[v[j]])) : 0u;
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) {
+            stage_push(st, near[j], v[j], deg[j]);
+            stage_far(st, far[j], v[j], far[j] ? 0x7fffffff - __float_as_int(nd[j]) : 0);
+        }
+    }
+};
+
 // --------------------------------------------------------------- BFS kernel
 __global__ void __launch_bounds__(kBlock) bfs_persistent(TravArgs a)
 {
     __shared__ TileShared ts;
+    __shared__ Stage st;
     __shared__ int s_dir;
     Ctl *ctl = a.ctl;
     const int gtid = blockIdx.x * kBlock + threadIdx.x, nth = gridDim.x * kBlock;
-    const unsigned gwarp = gtid >> 5, nwarps = nth >> 5;
+    const unsigned gwarp = gtid >> 5, nwarps = nth >> 5, wic = threadIdx.x >> 5;
     const int s = a.source;
     int ph = 0;
 
+    stage_init(st);
     for (int v = gtid; v < a.V; v += nth) reinterpret_cast<int *>(a.value)[v] = v == s ? 0 : -1;
     for (int w = gtid; w < a.W; w += nth) a.visited[w] = w == (s >> 5) ? 1u << (s & 31) : 0u;
-    if (gtid == 0) a.q0[0] = s;
+    unsigned nq, nch;
+    seed_frontier(a, s, a.q0, a.chunks0, nq, nch);
     if (!grid_sync(ctl, a.timeout_ns, ph)) return;
     ph++;
+    if (gtid == 0) ctl->t0_ns = globaltimer();
 
     const unsigned long long deg_s = (unsigned long long)(__ldg(&a.out_off[s + 1]) - __ldg(&a.out_off[s]));
-    unsigned long long qlen = 1, nf_prev = 0, mf = deg_s, mu = (unsigned long long)a.E - deg_s;
+    unsigned long long nf = 1, nf_prev = 0, mf = deg_s, mu = (unsigned long long)a.E - deg_s;
     int dir = 0, prev_dir = 0, L = 0, cur = 0, fcur = 0, bu_steps = 0;
-    while (qlen > 0) {
+    while (nf > 0) {
         if (L >= a.max_steps) {
             if (gtid == 0) atomicCAS(&ctl->err, 0, kErrBudget);
             return;
@@ -362,91 +691,82 @@ __global__ void __launch_bounds__(kBlock) bfs_persistent(TravArgs a)
         if (threadIdx.x < 32) {
             int d = dir;
             if (a.force_dir >= 0) d = (L == 0) ? 0 : a.force_dir;
-            else if (a.mlp) d = mlp_argmax_warp(a.mlp, bfs_features(L, qlen, mf, mu, nf_prev, a.V, a.E, prev_dir), kBfsOut);
+            else if (a.mlp) d = mlp_argmax_warp(a.mlp, bfs_features(L, nf, mf, mu, nf_prev, a.V, a.E, prev_dir), kBfsOut);
             else if (dir == 0) { if ((double)mf > (double)mu / a.alpha) d = 1; }
-            else if (!(qlen >= nf_prev || (double)qlen > (double)a.V / a.beta)) d = 0;
+            else if (!(nf >= nf_prev || (double)nf > (double)a.V / a.beta)) d = 0;
             if (threadIdx.x == 0) s_dir = d;
         }
         __syncthreads();
         dir = s_dir;
         if (gtid == 0 && L < kMaxTrace) {
             ctl->dirs[L] = (unsigned char)dir;
-            ctl->frontier[L] = (unsigned)qlen;
+            ctl->frontier[L] = (unsigned)nf;
         }
-        const int32_t *q = cur ? a.q1 : a.q0;
-        int32_t *qn = cur ? a.q0 : a.q1;
-        unsigned long long qnext, mfn;
-        if (dir == 0) {
+        if (dir == 1 && prev_dir == 0) {
+            // frontier bitmap from the levels: bit v = (level[v] == L)
             clear_ahead(ctl, ph);
-            BfsTopDown vis{&a, L + 1, qn, 0u, &ctl->slot[ph % kSlots]};
-            expand_tiles(a, q, (unsigned)qlen, vis, ts, &ctl->slot[ph % kSlots]);
-            if (!grid_sync(ctl, a.timeout_ns, ph)) return;
-            SlotView s0 = read_slot(ctl, ph);
-            ph++;
-            clear_ahead(ctl, ph);
-            vis.qbase = s0.q_add;
-            vis.slot = &ctl->slot[ph % kSlots];
-            expand_chunks(a, s0.chunk_add, vis);
-            if (!grid_sync(ctl, a.timeout_ns, ph)) return;
-            SlotView s1 = read_slot(ctl, ph);
-            ph++;
-            qnext = (unsigned long long)s0.q_add + s1.q_add;
-            mfn = s0.mf + s1.mf;
-        } else {
-            unsigned *fc = fcur ? a.front1 : a.front0;
-            unsigned *fn = fcur ? a.front0 : a.front1;
-            if (prev_dir == 0) {
-                // frontier bitmap from the levels: bit v = (level[v] == L)
-                clear_ahead(ctl, ph);
-                for (unsigned w = gwarp; w < (unsigned)a.W; w += nwarps) {
-                    int v = (int)(w * 32 + lane_id());
-                    bool f = v < a.V && (int)__ldcg(&a.value[v]) == L;
-                    unsigned m = __ballot_sync(kFull, f);
-                    if (lane_id() == 0) fc[w] = m;
-                }
-                if (!grid_sync(ctl, a.timeout_ns, ph)) return;
-                ph++;
-            }
-            clear_ahead(ctl, ph);
-            Slot *slot = &ctl->slot[ph % kSlots];
-            // bottom-up: each warp owns 32 vertices = one bitmap word
             for (unsigned w = gwarp; w < (unsigned)a.W; w += nwarps) {
-                int v = (int)(w * 32 + lane_id());
-                unsigned vis = __ldcg(&a.visited[w]);
-                bool found = false;
-                if (v < a.V && !((vis >> lane_id()) & 1u)) {
-                    int k = __ldg(&a.in_off[v]);
-                    const int kend = __ldg(&a.in_off[v + 1]);
-                    for (; k < kend; k++) {
-                        int u = __ldg(&a.in_adj[k]);
-                        if ((__ldcg(&fc[u >> 5]) >> (u & 31)) & 1u) { found = true; break; }
-                    }
-                }
-                unsigned m = __ballot_sync(kFull, found);
-                if (lane_id() == 0) {
-                    fn[w] = m;
-                    if (m) a.visited[w] = vis | m;
-                }
-                unsigned deg = 0;
-                if (found) {
-                    reinterpret_cast<int *>(a.value)[v] = L + 1;
-                    deg = (unsigned)(__ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v]));
-                }
-                warp_append(found, v, qn, 0u, &slot->q_add);
-                warp_add_u64(deg, &slot->mf);
+                const int v = (int)(w * 32 + lane_id());
+                const bool f = v < a.V && (int)__ldcg(&a.value[v]) == L;
+                const unsigned m = __ballot_sync(kFull, f);
+                if (lane_id() == 0) (fcur ? a.front1 : a.front0)[w] = m;
             }
             if (!grid_sync(ctl, a.timeout_ns, ph)) return;
-            SlotView s0 = read_slot(ctl, ph);
+            log_phase(ctl, 2, (unsigned)nf);
             ph++;
-            qnext = s0.q_add;
-            mfn = s0.mf;
+        }
+        clear_ahead(ctl, ph);
+        const FrontierOut out{(cur ? a.q0 : a.q1), (cur ? a.chunks0 : a.chunks1), nullptr, 0u, &ctl->slot[ph % kSlots]};
+        if (dir == 0) {
+            const BfsPush vis{&a, L + 1};
+            expand_frontier(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, ts, st, out);
+        } else {
+            // bottom-up: each warp owns 32 vertices = one bitmap word; kWarps words per CTA iteration
+            const unsigned *fc = fcur ? a.front1 : a.front0;
+            unsigned *fn = fcur ? a.front0 : a.front1;
+            for (unsigned w0 = blockIdx.x * kWarps; w0 < (unsigned)a.W; w0 += gridDim.x * kWarps) {
+                const unsigned w = w0 + wic;
+                if (w < (unsigned)a.W) {
+                    const int v = (int)(w * 32 + lane_id());
+                    const unsigned vis = __ldcg(&a.visited[w]);
+                    bool found = false;
+                    if (v < a.V && !((vis >> lane_id()) & 1u)) {
+                        int k = __ldg(&a.in_off[v]);
+                        const int kend = __ldg(&a.in_off[v + 1]);
+                        for (; k < kend; k++) {
+                            const int u = __ldg(&a.in_adj[k]);
+                            if ((__ldcg(&fc[u >> 5]) >> (u & 31)) & 1u) { found = true; break; }
+                        }
+                    }
+                    const unsigned m = __ballot_sync(kFull, found);
+                    if (lane_id() == 0) {
+                        fn[w] = m;
+                        if (m) a.visited[w] = vis | m;
+                    }
+                    unsigned deg = 0;
+                    if (found) {
+                        reinterpret_cast<int *>(a.value)[v] = L + 1;
+                        deg = (unsigned)(__ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v]));
+                    }
+                    stage_push(st, found, v, deg);
+                    stage_add_mf(st, deg);
+                }
+                stage_flush(a, st, ts, out, false);
+            }
+            stage_flush(a, st, ts, out, true);
             fcur ^= 1;
             bu_steps++;
         }
-        mu -= mfn;
-        nf_prev = qlen;
-        qlen = qnext;
-        mf = mfn;
+        if (!grid_sync(ctl, a.timeout_ns, ph)) return;
+        log_phase(ctl, dir, (unsigned)nf);
+        const SlotView s0 = read_slot(ctl, ph);
+        ph++;
+        nq = s0.q_add;
+        nch = s0.chunk_add;
+        mu -= s0.mf;
+        nf_prev = nf;
+        nf = (unsigned long long)s0.q_add + s0.big_add;
+        mf = s0.mf;
         prev_dir = dir;
         L++;
         cur ^= 1;
@@ -460,20 +780,22 @@ __global__ void __launch_bounds__(kBlock) bfs_persistent(TravArgs a)
 }
 
 // -------------------------------------------------------------- SSSP kernel
-// Near/far delta-stepping: the near queue holds vertices whose distance
+// Near/far delta-stepping: the near frontier holds vertices whose distance
 // improved below the bucket bound `thr`; improvements at or above it go to
-// the far pile.  When the near queue drains, the bound advances and the far
-// pile is split (entries below the new bound move to the near queue, stale
-// ones are dropped).  delta = +inf gives Bellman-Ford over active vertices.
-// Any order of relaxations reaches the same fixpoint bits: fl(x + w) is
-// monotone in x and not below x for w >= 0.
+// the far pile.  When the near frontier drains, the bound advances and the
+// far pile is split (entries below the new bound move to the near frontier,
+// stale ones are dropped).  delta = +inf gives Bellman-Ford over active
+// vertices.  Any order of relaxations reaches the same fixpoint bits:
+// fl(x + w) is monotone in x and not below x for w >= 0.
 __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
 {
     __shared__ TileShared ts;
+    __shared__ Stage st;
     __shared__ float s_delta;
     Ctl *ctl = a.ctl;
     const int gtid = blockIdx.x * kBlock + threadIdx.x, nth = gridDim.x * kBlock;
     int ph = 0;
+    stage_init(st);
     // Stamp ids continue across queries so the stamp arrays need no clearing;
     // every CTA reads the base before the first barrier, thread 0 of CTA 0
     // advances it after the last one.  Near the int range they are recycled.
@@ -486,69 +808,69 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
         first_id = 0;
     }
     int near_id = first_id, far_id = first_id;
-    unsigned long long qlen, far_len = 0;
+    unsigned nq, nch, nbig;
+    unsigned long long far_len = 0;
     int min_far = (int)kFltMaxBits;
     float thr = a.delta > 0.0f ? a.delta : INFINITY;
 
     if (a.source >= 0) {
         const int s = a.source;
         for (int v = gtid; v < a.V; v += nth) a.value[v] = v == s ? 0u : kFltMaxBits;
-        if (gtid == 0) {
-            a.q0[0] = s;
-            a.stamp_near[s] = near_id;
-        }
+        seed_frontier(a, s, a.q0, a.chunks0, nq, nch);
+        nbig = nch ? 1u : 0u;
+        if (gtid == 0) a.stamp_near[s] = near_id;
         if (!grid_sync(ctl, a.timeout_ns, ph)) return;
         ph++;
-        qlen = 1;
+        if (gtid == 0) ctl->t0_ns = globaltimer();
     } else {
         // start from the distances already in `value` (Bellman-Ford entry
         // point): every vertex below FLT_MAX is active.
         thr = INFINITY;
         clear_ahead(ctl, ph);
-        Slot *slot = &ctl->slot[ph % kSlots];
-        for (int base = gtid - (int)lane_id(); base < a.V; base += nth) {
-            int v = base + (int)lane_id();
-            bool act = v < a.V && __ldcg(&a.value[v]) < kFltMaxBits;
+        const FrontierOut out{a.q0, a.chunks0, nullptr, 0u, &ctl->slot[ph % kSlots]};
+        for (int base = blockIdx.x * kBlock; base < a.V; base += gridDim.x * kBlock) {
+            const int v = base + (int)threadIdx.x;
+            const bool act = v < a.V && __ldcg(&a.value[v]) < kFltMaxBits;
             if (act) a.stamp_near[v] = near_id;
-            warp_append(act, v, a.q0, 0u, &slot->q_add);
+            const unsigned deg = act ? (unsigned)(__ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v])) : 0u;
+            stage_push(st, act, v, deg);
+            stage_flush(a, st, ts, out, false);
         }
+        stage_flush(a, st, ts, out, true);
         if (!grid_sync(ctl, a.timeout_ns, ph)) return;
-        qlen = read_slot(ctl, ph).q_add;
+        const SlotView s0 = read_slot(ctl, ph);
+        nq = s0.q_add;
+        nch = s0.chunk_add;
+        nbig = s0.big_add;
         ph++;
+        if (gtid == 0) ctl->t0_ns = globaltimer();
     }
 
     int cur = 0, fcur = 0, steps = 0, buckets = 1;
-    float dcur = thr;  // width of the current bucket
     while (true) {
-        if (qlen > 0) {
+        if (nq + nch > 0) {
             if (steps >= a.max_steps) {
                 if (gtid == 0) atomicCAS(&ctl->err, 0, kErrBudget);
                 return;
             }
-            const int32_t *q = cur ? a.q1 : a.q0;
-            int32_t *qn = cur ? a.q0 : a.q1;
-            int32_t *fp = fcur ? a.far1 : a.far0;
             clear_ahead(ctl, ph);
-            SsspRelax vis{&a, thr, near_id + 1, far_id, qn, 0u, fp, (unsigned)far_len, &ctl->slot[ph % kSlots]};
-            expand_tiles(a, q, (unsigned)qlen, vis, ts, &ctl->slot[ph % kSlots]);
+            const FrontierOut out{(cur ? a.q0 : a.q1), (cur ? a.chunks0 : a.chunks1), (fcur ? a.far1 : a.far0),
+                                  (unsigned)far_len, &ctl->slot[ph % kSlots]};
+            const SsspPush vis{&a, thr, near_id + 1, far_id};
+            expand_frontier(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, ts, st, out);
             if (!grid_sync(ctl, a.timeout_ns, ph)) return;
-            SlotView s0 = read_slot(ctl, ph);
+            log_phase(ctl, 3, nq + nbig);
+            const SlotView s0 = read_slot(ctl, ph);
             ph++;
-            clear_ahead(ctl, ph);
-            vis.qbase = s0.q_add;
-            vis.fbase = (unsigned)(far_len + s0.far_add);
-            vis.slot = &ctl->slot[ph % kSlots];
-            expand_chunks(a, s0.chunk_add, vis);
-            if (!grid_sync(ctl, a.timeout_ns, ph)) return;
-            SlotView s1 = read_slot(ctl, ph);
-            ph++;
-            qlen = (unsigned long long)s0.q_add + s1.q_add;
-            far_len += (unsigned long long)s0.far_add + s1.far_add;
-            min_far = min(min_far, min(s0.min_far_bits, s1.min_far_bits));
+            if (gtid == 0 && steps < kMaxTrace) ctl->frontier[steps] = nq + nbig;
+            nq = s0.q_add;
+            nch = s0.chunk_add;
+            nbig = s0.big_add;
+            far_len += s0.far_add;
+            min_far = min(min_far, s0.min_far_bits);
             near_id++;
             cur ^= 1;
             steps++;
-            if (gtid == 0 && steps - 1 < kMaxTrace) ctl->frontier[steps - 1] = (unsigned)qlen;
         } else if (far_len > 0) {
             if (buckets >= a.max_steps) {
                 if (gtid == 0) atomicCAS(&ctl->err, 0, kErrBudget);
@@ -564,33 +886,37 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
                 if (threadIdx.x == 0) s_delta = d;
             }
             __syncthreads();
-            dcur = s_delta;
+            const float width = s_delta;
             const float told = thr;
-            thr = __fadd_rn(fmaxf(told, __int_as_float(min_far)), dcur);
+            thr = __fadd_rn(fmaxf(told, __int_as_float(min_far)), width);
             if (!(thr > told)) thr = nextafterf(told, INFINITY);
             far_id++;
             const int32_t *fp = fcur ? a.far1 : a.far0;
-            int32_t *fq = fcur ? a.far0 : a.far1;
-            int32_t *q = cur ? a.q1 : a.q0;  // the (empty) current near queue
             clear_ahead(ctl, ph);
-            Slot *slot = &ctl->slot[ph % kSlots];
-            for (unsigned long long base = gtid - lane_id(); base < far_len; base += nth) {
-                unsigned long long i = base + lane_id();
-                bool valid = i < far_len;
-                int v = valid ? __ldcg(&fp[i]) : 0;
-                float d = valid ? __uint_as_float(__ldcg(&a.value[v])) : 0.0f;
-                bool to_near = valid && d >= told && d < thr && atomicExch(&a.stamp_near[v], near_id) != near_id;
-                bool keep = valid && d >= thr && atomicExch(&a.stamp_far[v], far_id) != far_id;
-                warp_append(to_near, v, q, 0u, &slot->q_add);
-                warp_append(keep, v, fq, 0u, &slot->far_add);
-                int key = keep ? 0x7fffffff - __float_as_int(d) : 0;
-                key = __reduce_max_sync(kFull, key);
-                if (key && lane_id() == 0) atomicMax(&slot->min_far_bits, key);
+            // the (empty) current near frontier receives the entries of the new bucket
+            const FrontierOut out{(cur ? a.q1 : a.q0), (cur ? a.chunks1 : a.chunks0), (fcur ? a.far0 : a.far1), 0u,
+                                  &ctl->slot[ph % kSlots]};
+            for (unsigned long long base = (unsigned long long)blockIdx.x * kBlock; base < far_len;
+                 base += (unsigned long long)gridDim.x * kBlock) {
+                const unsigned long long i = base + threadIdx.x;
+                const bool valid = i < far_len;
+                const int v = valid ? __ldcg(&fp[i]) : 0;
+                const float d = valid ? __uint_as_float(__ldcg(&a.value[v])) : 0.0f;
+                const bool to_near = valid && d >= told && d < thr && atomicExch(&a.stamp_near[v], near_id) != near_id;
+                const bool keep = valid && d >= thr && atomicExch(&a.stamp_far[v], far_id) != far_id;
+                const unsigned deg = to_near ? (unsigned)(__ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v])) : 0u;
+                stage_push(st, to_near, v, deg);
+                stage_far(st, keep, v, keep ? 0x7fffffff - __float_as_int(d) : 0);
+                stage_flush(a, st, ts, out, false);
             }
+            stage_flush(a, st, ts, out, true);
             if (!grid_sync(ctl, a.timeout_ns, ph)) return;
-            SlotView s0 = read_slot(ctl, ph);
+            log_phase(ctl, 4, (unsigned)far_len);
+            const SlotView s0 = read_slot(ctl, ph);
             ph++;
-            qlen = s0.q_add;
+            nq = s0.q_add;
+            nch = s0.chunk_add;
+            nbig = s0.big_add;
             far_len = s0.far_add;
             min_far = s0.min_far_bits;
             fcur ^= 1;
@@ -749,7 +1075,7 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
     const int64_t V = g.V > 0 ? g.V : 1;
     const int64_t W = (V + 31) / 32;
     ws->V = g.V;
-    ws->chunk_cap = V + g.E / kChunk + 1;
+    ws->chunk_cap = V + g.E / kItem + 1;
     TRY_CUDA(cudaMalloc(&ws->value, sizeof(unsigned) * V));
     TRY_CUDA(cudaMalloc(&ws->visited, sizeof(unsigned) * W));
     TRY_CUDA(cudaMalloc(&ws->front[0], sizeof(unsigned) * W));
@@ -760,7 +1086,8 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
     }
     TRY_CUDA(cudaMalloc(&ws->stamp_near, sizeof(int32_t) * V));
     TRY_CUDA(cudaMalloc(&ws->stamp_far, sizeof(int32_t) * V));
-    TRY_CUDA(cudaMalloc(&ws->chunks, sizeof(int2) * ws->chunk_cap));
+    TRY_CUDA(cudaMalloc(&ws->chunks[0], sizeof(int2) * ws->chunk_cap));
+    TRY_CUDA(cudaMalloc(&ws->chunks[1], sizeof(int2) * ws->chunk_cap));
     TRY_CUDA(cudaMalloc(&ws->ctl, sizeof(Ctl) * (size_t)nqueries));
     ws->ctl_cap = nqueries;
     TRY_CUDA(cudaMalloc(&ws->id_base, sizeof(int)));
@@ -782,7 +1109,8 @@ void workspace_free(Workspace *ws)
     }
     cudaFree(ws->stamp_near);
     cudaFree(ws->stamp_far);
-    cudaFree(ws->chunks);
+    cudaFree(ws->chunks[0]);
+    cudaFree(ws->chunks[1]);
     cudaFree(ws->ctl);
     cudaFree(ws->id_base);
     *ws = Workspace{};
@@ -810,7 +1138,9 @@ static TravArgs make_args(const DevGraph &g, Workspace *ws)
     a.far1 = ws->far[1];
     a.stamp_near = ws->stamp_near;
     a.stamp_far = ws->stamp_far;
-    a.chunks = ws->chunks;
+    a.chunks = ws->chunks[0];
+    a.chunks0 = ws->chunks[0];
+    a.chunks1 = ws->chunks[1];
     a.id_base = ws->id_base;
     a.timeout_ns = 10ull * 1000000000ull;
     return a;

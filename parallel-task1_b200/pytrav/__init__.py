@@ -46,7 +46,7 @@ EXPORTS = [
     "trav_bfs", "trav_sssp", "trav_last_stats", "trav_last_bfs_trace", "trav_init_distances_f32",
     "trav_bellman_ford_el_f32", "trav_bfs_el", "trav_el_file_read", "trav_el_file_write", "trav_mlp_set",
     "trav_mlp_param_count", "trav_last_error", "trav_version", "trav_last_batch_ms", "trav_graph_set_stream",
-    "trav_bfs_csr_noalloc",
+    "trav_bfs_csr_noalloc", "trav_last_phase_log",
 ]
 
 
@@ -67,7 +67,7 @@ class SsspOpts(C.Structure):
 class QueryStats(C.Structure):
     _fields_ = [("kind", C.c_int32), ("steps", C.c_int32), ("buckets", C.c_int32), ("bottom_up_steps", C.c_int32),
                 ("reached", C.c_int64), ("reached_edges", C.c_int64), ("algorithmic_bytes", C.c_int64),
-                ("kernel_ms", C.c_float)]
+                ("kernel_ms", C.c_float), ("edges_scanned", C.c_int64)]
 
 
 _lib = None
@@ -102,6 +102,7 @@ def lib():
         L.trav_last_batch_ms.argtypes = [vp, vp, i32, C.POINTER(i32)]
         L.trav_graph_set_stream.argtypes = [vp, vp]
         L.trav_bfs_csr_noalloc.argtypes = [vp, vp, i32, i64, i32, vp, vp]
+        L.trav_last_phase_log.argtypes = [vp, vp, vp, vp, vp, i32, C.POINTER(i32)]
         _lib = L
     return _lib
 
@@ -134,6 +135,7 @@ class Stats:
     reached_edges: int
     algorithmic_bytes: int
     kernel_ms: float
+    edges_scanned: int
 
 
 class Graph:
@@ -212,7 +214,7 @@ class Graph:
         s = QueryStats()
         _check(lib().trav_last_stats(self._h, C.byref(s)))
         return Stats("bfs" if s.kind == 0 else "sssp", s.steps, s.buckets, s.bottom_up_steps, s.reached,
-                     s.reached_edges, s.algorithmic_bytes, s.kernel_ms)
+                     s.reached_edges, s.algorithmic_bytes, s.kernel_ms, s.edges_scanned)
 
     def last_bfs_trace(self):
         cap = 4096
@@ -235,6 +237,19 @@ class Graph:
         """Run queries on a CUDA stream (int handle or torch.cuda.Stream); None = the handle's own."""
         h = getattr(stream, "cuda_stream", stream)
         _check(lib().trav_graph_set_stream(self._h, C.c_void_p(h) if h else None))
+
+    def last_phase_log(self):
+        """Per-phase log of the last query: (kind, frontier size, end time us, cumulative edges expanded)."""
+        cap = 4096
+        kind = np.zeros(cap, np.uint8)
+        size = np.zeros(cap, np.int64)
+        end = np.zeros(cap, np.float64)
+        edges = np.zeros(cap, np.int64)
+        n = C.c_int32()
+        _check(lib().trav_last_phase_log(self._h, kind.ctypes.data, size.ctypes.data, end.ctypes.data,
+                                         edges.ctypes.data, cap, C.byref(n)))
+        k = min(n.value, cap)
+        return kind[:k].copy(), size[:k].copy(), end[:k].copy(), edges[:k].copy()
 
     def set_mlp(self, kind: int, params):
         p = np.ascontiguousarray(params, np.float32)
