@@ -234,12 +234,22 @@ static int cmp_deg_desc(const void *pa, const void *pb)
     return a < b ? -1 : (a > b);
 }
 
-typedef struct { int32_t key; int64_t e; } row_item;
+typedef struct { uint32_t key; int64_t e; } row_item;
 static int cmp_row_item(const void *pa, const void *pb)
 {
     const row_item *a = (const row_item *)pa, *b = (const row_item *)pb;
     if (a->key != b->key) return a->key < b->key ? -1 : 1;
     return a->e < b->e ? -1 : (a->e > b->e);
+}
+
+/* Weight sort key: the bit pattern of a non-negative float orders like its
+ * value; -0.0 is taken as +0.0. */
+static uint32_t weight_key(float w)
+{
+    uint32_t u;
+    if (w == 0.0f) w = 0.0f;
+    memcpy(&u, &w, 4);
+    return u;
 }
 
 void orc_device_layout(int32_t V, int64_t E, const int32_t *src, const int32_t *dst, const float *w,
@@ -254,7 +264,7 @@ void orc_device_layout(int32_t V, int64_t E, const int32_t *src, const int32_t *
     qsort(old_of_new, (size_t)V, sizeof(int32_t), cmp_deg_desc);
     for (int32_t r = 0; r < V; r++) new_of_old[old_of_new[r]] = r;
 
-    /* out rows: key = new dst, tie by edge order */
+    /* out rows: key = weight, tie by edge order; in rows: key = new src, tie by edge order */
     int64_t *ecount = (int64_t *)calloc((size_t)V + 1, sizeof(int64_t));
     int64_t *icount = (int64_t *)calloc((size_t)V + 1, sizeof(int64_t));
     for (int64_t e = 0; e < E; e++) {
@@ -272,10 +282,10 @@ void orc_device_layout(int32_t V, int64_t E, const int32_t *src, const int32_t *
     for (int64_t e = 0; e < E; e++) {
         int32_t s = new_of_old[src[e]], t = new_of_old[dst[e]];
         int64_t k = ecount[s]++;
-        oitems[k].key = t;
+        oitems[k].key = weight_key(w[e]);
         oitems[k].e = e;
         int64_t j = icount[t]++;
-        iitems[j].key = s;
+        iitems[j].key = (uint32_t)s;
         iitems[j].e = e;
     }
     for (int32_t v = 0; v < V; v++) {
@@ -283,9 +293,10 @@ void orc_device_layout(int32_t V, int64_t E, const int32_t *src, const int32_t *
         qsort(iitems + in_off[v], (size_t)(in_off[v + 1] - in_off[v]), sizeof(row_item), cmp_row_item);
     }
     for (int64_t k = 0; k < E; k++) {
-        out_adj[k] = oitems[k].key;
-        out_w[k] = w[oitems[k].e];
-        in_adj[k] = iitems[k].key;
+        const int64_t e = oitems[k].e;
+        out_adj[k] = new_of_old[dst[e]];
+        out_w[k] = w[e] == 0.0f ? 0.0f : w[e];
+        in_adj[k] = (int32_t)iitems[k].key;
     }
     free(oitems);
     free(iitems);

@@ -49,7 +49,8 @@ void orc_build_csr(int32_t V, int64_t E, const int32_t *src, const int32_t *dst,
 int orc_bfs_levels(int32_t V, const int64_t *offsets, const int32_t *adj, int32_t source, int32_t *levels);
 
 /* Device layout restated for checking the ingest path: vertices relabelled by
- * out-degree descending (ties by id), rows sorted by (neighbour, edge order).
+ * out-degree descending (ties by id); out rows sorted by (weight, edge order)
+ * with -0.0 stored as +0.0; in rows sorted by (neighbour, edge order).
  * new_of_old / old_of_new have V entries; out_off/in_off V+1; out_adj, out_w,
  * in_adj E. */
 void orc_device_layout(int32_t V, int64_t E, const int32_t *src, const int32_t *dst, const float *w,

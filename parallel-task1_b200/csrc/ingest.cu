@@ -138,17 +138,28 @@ __global__ void relabel_kernel(int32_t V, const int32_t *__restrict__ old_of_new
     }
 }
 
+// Out-row key (new source, weight bits): rows sorted by weight so the edges
+// lighter than any delta form a prefix.  -0.0 is stored as +0.0 (the sum
+// d + w is the same for d >= 0) so that zero weights sort first.
 __global__ void edge_keys_kernel(int64_t E, int lv, const int32_t *__restrict__ src, const int32_t *__restrict__ dst,
                                  const int32_t *__restrict__ new_of_old, const float *__restrict__ w,
                                  unsigned long long *__restrict__ out_keys, unsigned long long *__restrict__ in_keys,
-                                 float *__restrict__ wv)
+                                 int32_t *__restrict__ out_dst)
 {
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
         unsigned long long s = (unsigned)new_of_old[src[e]], t = (unsigned)new_of_old[dst[e]];
-        out_keys[e] = (s << lv) | t;
+        float wt = w ? w[e] : 1.0f;
+        if (wt == 0.0f) wt = 0.0f;
+        out_keys[e] = (s << 32) | __float_as_uint(wt);
         in_keys[e] = (t << lv) | s;
-        wv[e] = w ? w[e] : 1.0f;
+        out_dst[e] = (int32_t)t;
     }
+}
+
+__global__ void low_word_float_kernel(int64_t E, const unsigned long long *__restrict__ keys, float *__restrict__ out)
+{
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x)
+        out[e] = __uint_as_float((unsigned)(keys[e] & 0xffffffffull));
 }
 
 __global__ void low_bits_kernel(int64_t E, unsigned long long mask, const unsigned long long *__restrict__ keys,
@@ -273,7 +284,8 @@ int build_graph_device(int32_t V, int64_t E, const int32_t *d_src, const int32_t
 
     DBuf<int32_t> out_deg, in_deg, ids, deg_sorted, out_deg_new, in_deg_new;
     DBuf<int32_t> out_off, in_off, new_of_old, old_of_new, out_adj, in_adj;
-    DBuf<float> out_w, wv;
+    DBuf<float> out_w;
+    DBuf<int32_t> dv;
     DBuf<unsigned long long> okeys, ikeys, skeys;
     TRY_CUDA(out_deg.alloc(V));
     TRY_CUDA(in_deg.alloc(V));
@@ -303,8 +315,8 @@ int build_graph_device(int32_t V, int64_t E, const int32_t *d_src, const int32_t
     size_t tb3 = 0, tb4 = 0;
     if (E > 0) {
         TRY_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb3, (unsigned long long *)nullptr,
-                                                 (unsigned long long *)nullptr, (float *)nullptr, (float *)nullptr,
-                                                 (int)E, 0, 2 * lv, st));
+                                                 (unsigned long long *)nullptr, (int32_t *)nullptr, (int32_t *)nullptr,
+                                                 (int)E, 0, 32 + lv, st));
         TRY_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tb4, (unsigned long long *)nullptr,
                                                 (unsigned long long *)nullptr, (int)E, 0, 2 * lv, st));
     }
@@ -326,13 +338,13 @@ int build_graph_device(int32_t V, int64_t E, const int32_t *d_src, const int32_t
         TRY_CUDA(okeys.alloc(E));
         TRY_CUDA(ikeys.alloc(E));
         TRY_CUDA(skeys.alloc(E));
-        TRY_CUDA(wv.alloc(E));
-        edge_keys_kernel<<<grid_for(E), 256, 0, st>>>(E, lv, d_src, d_dst, new_of_old.p, d_w, okeys.p, ikeys.p, wv.p);
+        TRY_CUDA(dv.alloc(E));
+        edge_keys_kernel<<<grid_for(E), 256, 0, st>>>(E, lv, d_src, d_dst, new_of_old.p, d_w, okeys.p, ikeys.p, dv.p);
         TRY_CUDA(cudaGetLastError());
-        // Rows by (new source, new destination); stable, so duplicates keep
+        // Out rows by (new source, weight); stable, so equal weights keep
         // their edge-list order.
-        TRY_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, tb3, okeys.p, skeys.p, wv.p, out_w.p, (int)E, 0, 2 * lv, st));
-        low_bits_kernel<<<grid_for(E), 256, 0, st>>>(E, mask, skeys.p, out_adj.p);
+        TRY_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, tb3, okeys.p, skeys.p, dv.p, out_adj.p, (int)E, 0, 32 + lv, st));
+        low_word_float_kernel<<<grid_for(E), 256, 0, st>>>(E, skeys.p, out_w.p);
         TRY_CUDA(cub::DeviceRadixSort::SortKeys(temp.p, tb4, ikeys.p, skeys.p, (int)E, 0, 2 * lv, st));
         low_bits_kernel<<<grid_for(E), 256, 0, st>>>(E, mask, skeys.p, in_adj.p);
         TRY_CUDA(cudaGetLastError());

@@ -30,7 +30,9 @@ struct Slot {
     int min_far_bits;             // min distance bits pushed to the far pile
     unsigned long long mf;        // out-degree sum of newly reached vertices
     unsigned int big_add;         // vertices pushed as chunk items (rows longer than kSmallDeg)
-    unsigned int pad;
+    unsigned int hq_add;          // SSSP heavy list: short heavy parts appended
+    unsigned int hchunk_add;      // SSSP heavy list: chunk items appended
+    unsigned int hbig_add;        // SSSP heavy list: vertices pushed as chunk items
 };
 
 // Control block of one persistent launch (zeroed by the host before launch).
@@ -84,6 +86,11 @@ struct Workspace {
     int32_t *far[2] = {nullptr, nullptr};         // V each
     int32_t *stamp_near = nullptr;     // V
     int32_t *stamp_far = nullptr;      // V
+    int32_t *stamp_heavy = nullptr;    // V
+    int32_t *hq[2] = {nullptr, nullptr};  // SSSP heavy lists (short heavy parts), V each
+    int2 *hchunks[2] = {nullptr, nullptr};  // SSSP heavy lists (chunk items), chunk_cap each
+    int32_t *nlight = nullptr;         // V: out-edges lighter than nlight_delta (rows are sorted by weight)
+    float nlight_delta = -1.0f;        // delta nlight was counted for (< 0: none)
     int2 *chunks[2] = {nullptr, nullptr};  // chunk_cap items each (current / next frontier)
     Ctl *ctl = nullptr;                // ctl_cap control blocks: one per query of a batch
     int ctl_cap = 0;
@@ -108,7 +115,10 @@ struct TravArgs {
     unsigned int *front0, *front1;
     int32_t *q0, *q1;
     int32_t *far0, *far1;
-    int32_t *stamp_near, *stamp_far;
+    int32_t *stamp_near, *stamp_far, *stamp_heavy;
+    int32_t *hq0, *hq1;       // SSSP heavy lists
+    int2 *hch0, *hch1;
+    const int32_t *__restrict__ nlight;  // light-prefix length per vertex; nullptr = every edge is light
     int2 *chunks;          // chunk items (two-phase expansion)
     int2 *chunks0, *chunks1;  // chunk items of the current / next frontier (one-phase expansion)
     Ctl *ctl;

@@ -97,6 +97,7 @@ struct SlotView {
     int min_far_bits;  // kFltMaxBits when nothing was pushed
     unsigned long long mf;
     unsigned big_add;
+    unsigned hq_add, hchunk_add, hbig_add;
 };
 
 __device__ __forceinline__ SlotView read_slot(const Ctl *ctl, int ph)
@@ -110,6 +111,9 @@ __device__ __forceinline__ SlotView read_slot(const Ctl *ctl, int ph)
     v.min_far_bits = neg > 0 ? 0x7fffffff - neg : (int)kFltMaxBits;
     v.mf = s->mf;
     v.big_add = s->big_add;
+    v.hq_add = s->hq_add;
+    v.hchunk_add = s->hchunk_add;
+    v.hbig_add = s->hbig_add;
     return v;
 }
 
@@ -125,6 +129,9 @@ __device__ __forceinline__ void clear_ahead(Ctl *ctl, int ph)
         s->min_far_bits = 0;
         s->mf = 0;
         s->big_add = 0;
+        s->hq_add = 0;
+        s->hchunk_add = 0;
+        s->hbig_add = 0;
     }
 }
 
@@ -312,56 +319,75 @@ __device__ void write_back(const TravArgs &a)
 
 // ------------------------------------------------------ one-phase frontier
 // The next frontier is written in two parts while it is discovered: vertices
-// with at most kSmallDeg out-edges go to a queue that the next step expands
-// by CTA tiles; longer rows are cut into kItem-edge items, expanded one warp
-// per item.  Both parts are complete when the step's barrier passes, so a
-// step is one phase and one grid barrier, and the work of long rows is spread
-// over every warp of the grid.
+// whose row to expand has at most kSmallDeg edges go to a queue that the next
+// step expands by CTA tiles; longer rows are cut into kItem-edge items,
+// expanded one warp per item.  Both parts are complete when the step's
+// barrier passes, so a step is one phase and one grid barrier, and the work
+// of long rows is spread over every warp of the grid.
 //
 // Pushes are staged per CTA in shared memory and written out in bulk: one
-// global atomic reserves room for up to a few thousand entries, and the
+// global atomic reserves room for up to a thousand or more entries, and the
 // scalar counters (out-degree sums, scanned edges, far minimum) are reduced
 // per CTA per phase.  Without this every warp hit the same few counters and
 // serialised on one L2 slice.  All loops that push are CTA-uniform, so the
 // flush points can use __syncthreads.
+//
+// A push goes to one of two targets: target 0 is the next frontier (for SSSP
+// its rows are the light prefixes, w < delta), target 1 is the SSSP heavy list
+// (rows are the heavy suffixes).  Rows are sorted by weight, so both parts are
+// contiguous: [off[v], off[v] + nlight[v]) and [off[v] + nlight[v], off[v+1]).
 constexpr int kBatch = 4;                      // independent edges per lane per round
 constexpr int kRoundPush = kBlock * kBatch;    // most pushes a CTA makes between two flush points
-constexpr int kFlushQ = 2048, kFlushBig = 256, kFlushFar = 2048;
+constexpr int kFlushQ = 1024, kFlushBig = 128, kFlushFar = 1024;
+
+constexpr int kPartWhole = 0, kPartLight = 1, kPartHeavy = 2;
 
 struct Stage {
-    int q[kFlushQ + kRoundPush];
-    int big[kFlushBig + kRoundPush];
+    int q[2][kFlushQ + kRoundPush];
+    int big[2][kFlushBig + kRoundPush];
     int far[kFlushFar + kRoundPush];
-    unsigned nq, nbig, nfar;
-    unsigned base_q, base_far, base_items;
-    unsigned big_total;
+    unsigned nq[2], nbig[2], nfar;
+    unsigned base_q[2], base_far, base_items;
+    unsigned big_total[2];
     int far_key;
     unsigned long long mf, scanned;
 };
 
 // Destination of one phase's pushes.
 struct FrontierOut {
-    int32_t *q;      // short-row queue of the next frontier
-    int2 *chunks;    // chunk items of the next frontier
-    int32_t *farp;   // far pile (SSSP)
-    unsigned fbase;  // far entries already in the pile before this phase
+    int32_t *q[2];       // short-row queues of the two targets
+    int2 *chunks[2];     // chunk items of the two targets
+    unsigned qbase[2];   // entries already in each target before this phase
+    unsigned cbase[2];
+    int part[2];         // which part of a row each target expands
+    int32_t *farp;       // far pile (SSSP)
+    unsigned fbase;      // far entries already in the pile before this phase
     Slot *slot;
 };
+
+// Row part [begin, end) of vertex v.
+__device__ __forceinline__ int2 row_part(const TravArgs &a, int v, int part)
+{
+    int rb = __ldg(&a.out_off[v]), re = __ldg(&a.out_off[v + 1]);
+    if (part == kPartLight) re = rb + __ldg(&a.nlight[v]);
+    else if (part == kPartHeavy) rb += __ldg(&a.nlight[v]);
+    return make_int2(rb, re);
+}
 
 __device__ __forceinline__ void stage_init(Stage &st)
 {
     if (threadIdx.x == 0) {
-        st.nq = st.nbig = st.nfar = 0;
-        st.big_total = 0;
+        st.nq[0] = st.nq[1] = st.nbig[0] = st.nbig[1] = st.nfar = 0;
+        st.big_total[0] = st.big_total[1] = 0;
         st.far_key = 0;
         st.mf = st.scanned = 0;
     }
     __syncthreads();
 }
 
-// Warp-collective: lanes with `flag` push vertex v whose row to expand next
-// has `len` edges (tile queue or chunk items by length).
-__device__ __forceinline__ void stage_push(Stage &st, bool flag, int v, unsigned len)
+// Warp-collective: lanes with `flag` push vertex v to target t; `len` is the
+// length of the row part the target will expand (tile queue or chunk items).
+__device__ __forceinline__ void stage_push(Stage &st, int t, bool flag, int v, unsigned len)
 {
     const bool big = flag && len > (unsigned)kSmallDeg;
     const bool small = flag && !big;
@@ -369,19 +395,19 @@ __device__ __forceinline__ void stage_push(Stage &st, bool flag, int v, unsigned
     if (ms) {
         const unsigned leader = __ffs(ms) - 1;
         unsigned pos = 0;
-        if (lane_id() == leader) pos = atomicAdd(&st.nq, (unsigned)__popc(ms));
+        if (lane_id() == leader) pos = atomicAdd(&st.nq[t], (unsigned)__popc(ms));
         pos = __shfl_sync(kFull, pos, leader);
-        if (small) st.q[pos + __popc(ms & lanemask_lt())] = v;
+        if (small) st.q[t][pos + __popc(ms & lanemask_lt())] = v;
     }
     if (mb) {
         const unsigned leader = __ffs(mb) - 1;
         unsigned pos = 0;
         if (lane_id() == leader) {
-            pos = atomicAdd(&st.nbig, (unsigned)__popc(mb));
-            atomicAdd(&st.big_total, (unsigned)__popc(mb));
+            pos = atomicAdd(&st.nbig[t], (unsigned)__popc(mb));
+            atomicAdd(&st.big_total[t], (unsigned)__popc(mb));
         }
         pos = __shfl_sync(kFull, pos, leader);
-        if (big) st.big[pos + __popc(mb & lanemask_lt())] = v;
+        if (big) st.big[t][pos + __popc(mb & lanemask_lt())] = v;
     }
 }
 
@@ -411,61 +437,66 @@ __device__ __forceinline__ void stage_add_mf(Stage &st, unsigned x)
 __device__ void stage_flush(const TravArgs &a, Stage &st, TileShared &ts, const FrontierOut &o, bool final)
 {
     __syncthreads();
-    const unsigned nq = st.nq, nbig = st.nbig, nfar = st.nfar;
-    const bool dq = nq > 0 && (final || nq >= (unsigned)kFlushQ);
-    const bool db = nbig > 0 && (final || nbig >= (unsigned)kFlushBig);
-    const bool df = nfar > 0 && (final || nfar >= (unsigned)kFlushFar);
-    if (dq || db || df) {
-        if (threadIdx.x == 0) {
-            if (dq) st.base_q = atomicAdd(&o.slot->q_add, nq);
-            if (df) st.base_far = o.fbase + atomicAdd(&o.slot->far_add, nfar);
-        }
+    for (int t = 0; t < 2; t++) {
+        const unsigned nq = st.nq[t], nbig = st.nbig[t];
+        const bool dq = nq > 0 && (final || nq >= (unsigned)kFlushQ);
+        const bool db = nbig > 0 && (final || nbig >= (unsigned)kFlushBig);
+        if (!(dq || db)) continue;
+        if (dq && threadIdx.x == 0) st.base_q[t] = o.qbase[t] + atomicAdd(t ? &o.slot->hq_add : &o.slot->q_add, nq);
         if (db) {
             for (unsigned r = 0; r < nbig; r += kBlock) {
                 const unsigned i = r + threadIdx.x;
-                int v = 0, rb = 0, nch = 0;
+                int v = 0, nch = 0;
+                int2 p = make_int2(0, 0);
                 if (i < nbig) {
-                    v = st.big[i];
-                    rb = __ldg(&a.out_off[v]);
-                    nch = (__ldg(&a.out_off[v + 1]) - rb + kItem - 1) / kItem;
+                    v = st.big[t][i];
+                    p = row_part(a, v, o.part[t]);
+                    nch = (p.y - p.x + kItem - 1) / kItem;
                 }
                 const int pre = block_excl_scan(nch, ts);
-                if (threadIdx.x == 0) st.base_items = atomicAdd(&o.slot->chunk_add, (unsigned)ts.total);
+                if (threadIdx.x == 0)
+                    st.base_items = o.cbase[t] + atomicAdd(t ? &o.slot->hchunk_add : &o.slot->chunk_add, (unsigned)ts.total);
                 __syncthreads();
                 const unsigned base = st.base_items + (unsigned)pre;
-                for (int c = 0; c < nch; c++) o.chunks[base + c] = make_int2(v, rb + c * kItem);
+                for (int c = 0; c < nch; c++) o.chunks[t][base + c] = make_int2(v, p.x + c * kItem);
                 __syncthreads();
             }
         }
         __syncthreads();
         if (dq)
-            for (unsigned i = threadIdx.x; i < nq; i += kBlock) o.q[st.base_q + i] = st.q[i];
-        if (df)
-            for (unsigned i = threadIdx.x; i < nfar; i += kBlock) o.farp[st.base_far + i] = st.far[i];
+            for (unsigned i = threadIdx.x; i < nq; i += kBlock) o.q[t][st.base_q[t] + i] = st.q[t][i];
         __syncthreads();
         if (threadIdx.x == 0) {
-            if (dq) st.nq = 0;
-            if (db) st.nbig = 0;
-            if (df) st.nfar = 0;
+            if (dq) st.nq[t] = 0;
+            if (db) st.nbig[t] = 0;
         }
+    }
+    const unsigned nfar = st.nfar;
+    if (nfar > 0 && (final || nfar >= (unsigned)kFlushFar)) {
+        if (threadIdx.x == 0) st.base_far = o.fbase + atomicAdd(&o.slot->far_add, nfar);
+        __syncthreads();
+        for (unsigned i = threadIdx.x; i < nfar; i += kBlock) o.farp[st.base_far + i] = st.far[i];
+        __syncthreads();
+        if (threadIdx.x == 0) st.nfar = 0;
     }
     if (final && threadIdx.x == 0) {
         if (st.mf) atomicAdd(&o.slot->mf, st.mf);
         if (st.scanned) atomicAdd(&a.ctl->edges_scanned, st.scanned);
-        if (st.big_total) atomicAdd(&o.slot->big_add, st.big_total);
+        if (st.big_total[0]) atomicAdd(&o.slot->big_add, st.big_total[0]);
+        if (st.big_total[1]) atomicAdd(&o.slot->hbig_add, st.big_total[1]);
         if (st.far_key) atomicMax(&o.slot->min_far_bits, st.far_key);
         st.mf = st.scanned = 0;
-        st.big_total = 0;
+        st.big_total[0] = st.big_total[1] = 0;
         st.far_key = 0;
     }
     __syncthreads();
 }
 
-// Expand a frontier in one phase: chunk items (one warp each, kWarps items
-// per CTA iteration), then the short-row queue by CTA tiles (edge-balanced
-// within the tile).  Every lane carries kBatch independent edges per round so
-// their loads and atomics overlap.
-template <class Vis>
+// Expand a frontier (part kPart of each row) in one phase: chunk items (one
+// warp each, kWarps items per CTA iteration), then the short-row queue by CTA
+// tiles (edge-balanced within the tile).  Every lane carries kBatch
+// independent edges per round so their loads and atomics overlap.
+template <int kPart, class Vis>
 __device__ void expand_frontier(const TravArgs &a, const int32_t *q, unsigned nq, const int2 *chunks, unsigned nch,
                                 const Vis &vis, TileShared &ts, Stage &st, const FrontierOut &o)
 {
@@ -479,7 +510,7 @@ __device__ void expand_frontier(const TravArgs &a, const int32_t *q, unsigned nq
             const int2 it = __ldcg(&chunks[c]);
             u = it.x;
             start = it.y;
-            end = min(start + kItem, __ldg(&a.out_off[u + 1]));
+            end = min(start + kItem, row_part(a, u, kPart).y);
             du = vis.begin(u);
             if (lane == 0) atomicAdd(&st.scanned, (unsigned long long)(end - start));
         }
@@ -503,8 +534,9 @@ __device__ void expand_frontier(const TravArgs &a, const int32_t *q, unsigned nq
         int u = 0, rb = 0, deg = 0;
         if (i < nq) {
             u = __ldcg(&q[i]);
-            rb = __ldg(&a.out_off[u]);
-            deg = __ldg(&a.out_off[u + 1]) - rb;
+            const int2 p = row_part(a, u, kPart);
+            rb = p.x;
+            deg = p.y - p.x;
         }
         const int pre = block_excl_scan(deg, ts);
         ts.u[threadIdx.x] = u;
@@ -545,20 +577,19 @@ __device__ void expand_frontier(const TravArgs &a, const int32_t *q, unsigned nq
     stage_flush(a, st, ts, o, true);
 }
 
-// Single-source frontier: the source alone (every CTA computes the counts).
-__device__ __forceinline__ void seed_frontier(const TravArgs &a, int s, int32_t *q, int2 *chunks, unsigned &nq,
-                                              unsigned &nch)
+// One vertex as a frontier of its own (row part [rb, re)): every CTA computes
+// the counts; the items are written by the first threads of the grid.
+__device__ __forceinline__ void seed_part(int s, int rb, int re, int32_t *q, int2 *chunks, unsigned &nq, unsigned &nch)
 {
-    const int rb = __ldg(&a.out_off[s]);
-    const int deg = __ldg(&a.out_off[s + 1]) - rb;
     const int gtid = blockIdx.x * kBlock + threadIdx.x, nth = gridDim.x * kBlock;
-    if (deg > kSmallDeg) {
-        nq = 0;
-        nch = (unsigned)((deg + kItem - 1) / kItem);
+    const int len = re - rb;
+    nq = nch = 0;
+    if (len <= 0) return;
+    if (len > kSmallDeg) {
+        nch = (unsigned)((len + kItem - 1) / kItem);
         for (int c = gtid; c < (int)nch; c += nth) chunks[c] = make_int2(s, rb + c * kItem);
     } else {
         nq = 1;
-        nch = 0;
         if (gtid == 0) q[0] = s;
     }
 }
@@ -598,15 +629,20 @@ struct BfsPush {
             dsum += deg[j];
         }
 #pragma unroll
-        for (int j = 0; j < kBatch; j++) stage_push(st, fresh[j], v[j], deg[j]);
+        for (int j = 0; j < kBatch; j++) stage_push(st, 0, fresh[j], v[j], deg[j]);
         stage_add_mf(st, dsum);
     }
 };
 
+// SSSP relaxation.  An improvement below the bucket bound puts the vertex on
+// the next frontier (its light prefix, deduplicated by stamp_near) and, when
+// it has heavy edges, on the heavy list of the current round (deduplicated by
+// stamp_heavy); one at or above the bound goes to the far pile.
 struct SsspPush {
     const TravArgs *a;
     float thr;          // bucket upper bound (exclusive)
-    int near_id;        // stamp of the next near frontier
+    int near_id;        // stamp of the frontier being filled
+    int heavy_id;       // stamp of the heavy list being filled
     int far_id;         // stamp of the current far epoch
 
     __device__ __forceinline__ float begin(int u) const { return __uint_as_float(__ldcg(&a->value[u])); }
@@ -637,22 +673,33 @@ struct SsspPush {
                 imp[j] = nd[j] < __int_as_float(old);
             }
         }
-        bool near[kBatch], far[kBatch];
+        int nl[kBatch], nh[kBatch];
 #pragma unroll
         for (int j = 0; j < kBatch; j++) {
-            near[j] = far[j] = false;
-            if (imp[j]) {
-                if (nd[j] < thr) near[j] = atomicExch(&a->stamp_near[v[j]], near_id) != near_id;
-                else far[j] = atomicExch(&a->stamp_far[v[j]], far_id) != far_id;
+            nl[j] = nh[j] = 0;
+            if (imp[j] && nd[j] < thr) {
+                const int deg = __ldg(&a->out_off[v[j] + 1]) - __ldg(&a->out_off[v[j]]);
+                nl[j] = a->nlight ? __ldg(&a->nlight[v[j]]) : deg;
+                nh[j] = deg - nl[j];
             }
         }
-        unsigned deg[kBatch];
-#pragma unroll
-        for (int j = 0; j < kBatch; j++)
-            deg[j] = near[j] ? (unsigned)(__ldg(&a->out_off[v[j] + 1]) - __ldg(&a->out_off[v[j]])) : 0u;
+        bool light[kBatch], heavy[kBatch], far[kBatch];
 #pragma unroll
         for (int j = 0; j < kBatch; j++) {
-            stage_push(st, near[j], v[j], deg[j]);
+            light[j] = heavy[j] = far[j] = false;
+            if (imp[j]) {
+                if (nd[j] < thr) {
+                    if (nl[j] > 0) light[j] = atomicExch(&a->stamp_near[v[j]], near_id) != near_id;
+                    if (nh[j] > 0) heavy[j] = atomicExch(&a->stamp_heavy[v[j]], heavy_id) != heavy_id;
+                } else {
+                    far[j] = atomicExch(&a->stamp_far[v[j]], far_id) != far_id;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) {
+            stage_push(st, 0, light[j], v[j], (unsigned)nl[j]);
+            stage_push(st, 1, heavy[j], v[j], (unsigned)nh[j]);
             stage_far(st, far[j], v[j], far[j] ? 0x7fffffff - __float_as_int(nd[j]) : 0);
         }
     }
@@ -674,7 +721,7 @@ __global__ void __launch_bounds__(kBlock) bfs_persistent(TravArgs a)
     for (int v = gtid; v < a.V; v += nth) reinterpret_cast<int *>(a.value)[v] = v == s ? 0 : -1;
     for (int w = gtid; w < a.W; w += nth) a.visited[w] = w == (s >> 5) ? 1u << (s & 31) : 0u;
     unsigned nq, nch;
-    seed_frontier(a, s, a.q0, a.chunks0, nq, nch);
+    seed_part(s, __ldg(&a.out_off[s]), __ldg(&a.out_off[s + 1]), a.q0, a.chunks0, nq, nch);
     if (!grid_sync(ctl, a.timeout_ns, ph)) return;
     ph++;
     if (gtid == 0) ctl->t0_ns = globaltimer();
@@ -716,10 +763,11 @@ __global__ void __launch_bounds__(kBlock) bfs_persistent(TravArgs a)
             ph++;
         }
         clear_ahead(ctl, ph);
-        const FrontierOut out{(cur ? a.q0 : a.q1), (cur ? a.chunks0 : a.chunks1), nullptr, 0u, &ctl->slot[ph % kSlots]};
+        const FrontierOut out{{(cur ? a.q0 : a.q1), nullptr}, {(cur ? a.chunks0 : a.chunks1), nullptr}, {0u, 0u},
+                              {0u, 0u}, {kPartWhole, kPartWhole}, nullptr, 0u, &ctl->slot[ph % kSlots]};
         if (dir == 0) {
             const BfsPush vis{&a, L + 1};
-            expand_frontier(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, ts, st, out);
+            expand_frontier<kPartWhole>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, ts, st, out);
         } else {
             // bottom-up: each warp owns 32 vertices = one bitmap word; kWarps words per CTA iteration
             const unsigned *fc = fcur ? a.front1 : a.front0;
@@ -748,7 +796,7 @@ __global__ void __launch_bounds__(kBlock) bfs_persistent(TravArgs a)
                         reinterpret_cast<int *>(a.value)[v] = L + 1;
                         deg = (unsigned)(__ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v]));
                     }
-                    stage_push(st, found, v, deg);
+                    stage_push(st, 0, found, v, deg);
                     stage_add_mf(st, deg);
                 }
                 stage_flush(a, st, ts, out, false);
@@ -780,13 +828,20 @@ __global__ void __launch_bounds__(kBlock) bfs_persistent(TravArgs a)
 }
 
 // -------------------------------------------------------------- SSSP kernel
-// Near/far delta-stepping: the near frontier holds vertices whose distance
-// improved below the bucket bound `thr`; improvements at or above it go to
-// the far pile.  When the near frontier drains, the bound advances and the
-// far pile is split (entries below the new bound move to the near frontier,
-// stale ones are dropped).  delta = +inf gives Bellman-Ford over active
-// vertices.  Any order of relaxations reaches the same fixpoint bits:
-// fl(x + w) is monotone in x and not below x for w >= 0.
+// Delta-stepping with light and heavy edges over a near/far split.  Inside a
+// bucket [lo, thr), relaxation rounds expand only the light prefixes (w <
+// delta) of the frontier; improvements below thr feed the next round,
+// improvements at or above it go to the far pile.  Every vertex improved below
+// thr is also put (once per round of the heavy list) on the heavy list, whose
+// heavy suffixes are relaxed once the light rounds drain -- so a vertex whose
+// distance is corrected several times inside the bucket re-scans only its light
+// edges.  With width = delta a heavy edge always lands at or above thr; with a
+// wider bucket (the learned schedule) it may land below, and then its target
+// starts new light rounds and joins the next heavy list.  When the frontier
+// and the heavy list are empty the bound advances and the far pile is split.
+// delta = +inf is Bellman-Ford over active vertices (every edge light).  Any
+// order of relaxations reaches the same fixpoint bits: fl(x + w) is monotone
+// in x and not below x for w >= 0.
 __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
 {
     __shared__ TileShared ts;
@@ -794,6 +849,7 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
     __shared__ float s_delta;
     Ctl *ctl = a.ctl;
     const int gtid = blockIdx.x * kBlock + threadIdx.x, nth = gridDim.x * kBlock;
+    const int lpart = a.nlight ? kPartLight : kPartWhole;
     int ph = 0;
     stage_init(st);
     // Stamp ids continue across queries so the stamp arrays need no clearing;
@@ -804,36 +860,49 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
         for (int v = gtid; v < a.V; v += nth) {
             a.stamp_near[v] = -1;
             a.stamp_far[v] = -1;
+            a.stamp_heavy[v] = -1;
         }
         first_id = 0;
     }
-    int near_id = first_id, far_id = first_id;
-    unsigned nq, nch, nbig;
+    int near_id = first_id, far_id = first_id, heavy_id = first_id;
+    unsigned nq, nch, nbig;                 // current frontier (light parts)
+    unsigned hq = 0, hch = 0, hbig = 0;     // heavy list of the current round
     unsigned long long far_len = 0;
     int min_far = (int)kFltMaxBits;
     float thr = a.delta > 0.0f ? a.delta : INFINITY;
+    int cur = 0, hcur = 0, fcur = 0;
 
     if (a.source >= 0) {
         const int s = a.source;
         for (int v = gtid; v < a.V; v += nth) a.value[v] = v == s ? 0u : kFltMaxBits;
-        seed_frontier(a, s, a.q0, a.chunks0, nq, nch);
+        const int2 lp = row_part(a, s, lpart);
+        seed_part(s, lp.x, lp.y, a.q0, a.chunks0, nq, nch);
         nbig = nch ? 1u : 0u;
-        if (gtid == 0) a.stamp_near[s] = near_id;
+        if (a.nlight) {
+            const int2 hp = row_part(a, s, kPartHeavy);
+            seed_part(s, hp.x, hp.y, a.hq0, a.hch0, hq, hch);
+            hbig = hch ? 1u : 0u;
+        }
+        if (gtid == 0) {
+            a.stamp_near[s] = near_id;
+            a.stamp_heavy[s] = heavy_id;
+        }
         if (!grid_sync(ctl, a.timeout_ns, ph)) return;
         ph++;
         if (gtid == 0) ctl->t0_ns = globaltimer();
     } else {
         // start from the distances already in `value` (Bellman-Ford entry
-        // point): every vertex below FLT_MAX is active.
+        // point, every edge light): every vertex below FLT_MAX is active.
         thr = INFINITY;
         clear_ahead(ctl, ph);
-        const FrontierOut out{a.q0, a.chunks0, nullptr, 0u, &ctl->slot[ph % kSlots]};
+        const FrontierOut out{{a.q0, nullptr}, {a.chunks0, nullptr}, {0u, 0u}, {0u, 0u}, {kPartWhole, kPartWhole},
+                              nullptr, 0u, &ctl->slot[ph % kSlots]};
         for (int base = blockIdx.x * kBlock; base < a.V; base += gridDim.x * kBlock) {
             const int v = base + (int)threadIdx.x;
             const bool act = v < a.V && __ldcg(&a.value[v]) < kFltMaxBits;
             if (act) a.stamp_near[v] = near_id;
             const unsigned deg = act ? (unsigned)(__ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v])) : 0u;
-            stage_push(st, act, v, deg);
+            stage_push(st, 0, act && deg > 0, v, deg);
             stage_flush(a, st, ts, out, false);
         }
         stage_flush(a, st, ts, out, true);
@@ -846,18 +915,28 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
         if (gtid == 0) ctl->t0_ns = globaltimer();
     }
 
-    int cur = 0, fcur = 0, steps = 0, buckets = 1;
+    int steps = 0, buckets = 1;
     while (true) {
+        if (steps + buckets >= a.max_steps) {
+            if (gtid == 0) atomicCAS(&ctl->err, 0, kErrBudget);
+            return;
+        }
         if (nq + nch > 0) {
-            if (steps >= a.max_steps) {
-                if (gtid == 0) atomicCAS(&ctl->err, 0, kErrBudget);
-                return;
-            }
+            // light round: frontier (cur) -> next frontier (cur^1) + heavy list (hcur, appended)
             clear_ahead(ctl, ph);
-            const FrontierOut out{(cur ? a.q0 : a.q1), (cur ? a.chunks0 : a.chunks1), (fcur ? a.far1 : a.far0),
-                                  (unsigned)far_len, &ctl->slot[ph % kSlots]};
-            const SsspPush vis{&a, thr, near_id + 1, far_id};
-            expand_frontier(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, ts, st, out);
+            const FrontierOut out{{(cur ? a.q0 : a.q1), (hcur ? a.hq1 : a.hq0)},
+                                  {(cur ? a.chunks0 : a.chunks1), (hcur ? a.hch1 : a.hch0)},
+                                  {0u, hq},
+                                  {0u, hch},
+                                  {lpart, kPartHeavy},
+                                  (fcur ? a.far1 : a.far0),
+                                  (unsigned)far_len,
+                                  &ctl->slot[ph % kSlots]};
+            const SsspPush vis{&a, thr, near_id + 1, heavy_id, far_id};
+            if (lpart == kPartLight)
+                expand_frontier<kPartLight>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, ts, st, out);
+            else
+                expand_frontier<kPartWhole>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, ts, st, out);
             if (!grid_sync(ctl, a.timeout_ns, ph)) return;
             log_phase(ctl, 3, nq + nbig);
             const SlotView s0 = read_slot(ctl, ph);
@@ -866,16 +945,43 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
             nq = s0.q_add;
             nch = s0.chunk_add;
             nbig = s0.big_add;
+            hq += s0.hq_add;
+            hch += s0.hchunk_add;
+            hbig += s0.hbig_add;
             far_len += s0.far_add;
             min_far = min(min_far, s0.min_far_bits);
             near_id++;
             cur ^= 1;
             steps++;
+        } else if (hq + hch > 0) {
+            // heavy round: heavy list (hcur) -> frontier (cur, empty) + next heavy list (hcur^1)
+            clear_ahead(ctl, ph);
+            const FrontierOut out{{(cur ? a.q1 : a.q0), (hcur ? a.hq0 : a.hq1)},
+                                  {(cur ? a.chunks1 : a.chunks0), (hcur ? a.hch0 : a.hch1)},
+                                  {0u, 0u},
+                                  {0u, 0u},
+                                  {lpart, kPartHeavy},
+                                  (fcur ? a.far1 : a.far0),
+                                  (unsigned)far_len,
+                                  &ctl->slot[ph % kSlots]};
+            const SsspPush vis{&a, thr, near_id, heavy_id + 1, far_id};
+            expand_frontier<kPartHeavy>(a, (hcur ? a.hq1 : a.hq0), hq, (hcur ? a.hch1 : a.hch0), hch, vis, ts, st, out);
+            if (!grid_sync(ctl, a.timeout_ns, ph)) return;
+            log_phase(ctl, 5, hq + hbig);
+            const SlotView s0 = read_slot(ctl, ph);
+            ph++;
+            nq = s0.q_add;
+            nch = s0.chunk_add;
+            nbig = s0.big_add;
+            hq = s0.hq_add;
+            hch = s0.hchunk_add;
+            hbig = s0.hbig_add;
+            far_len += s0.far_add;
+            min_far = min(min_far, s0.min_far_bits);
+            heavy_id++;
+            hcur ^= 1;
+            steps++;
         } else if (far_len > 0) {
-            if (buckets >= a.max_steps) {
-                if (gtid == 0) atomicCAS(&ctl->err, 0, kErrBudget);
-                return;
-            }
             // open the next bucket (skipping empty ones): bound = max(old, min far) + width
             if (threadIdx.x < 32) {
                 float d = a.delta;
@@ -893,8 +999,14 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
             far_id++;
             const int32_t *fp = fcur ? a.far1 : a.far0;
             clear_ahead(ctl, ph);
-            // the (empty) current near frontier receives the entries of the new bucket
-            const FrontierOut out{(cur ? a.q1 : a.q0), (cur ? a.chunks1 : a.chunks0), (fcur ? a.far0 : a.far1), 0u,
+            // the (empty) frontier and heavy list receive the entries of the new bucket
+            const FrontierOut out{{(cur ? a.q1 : a.q0), (hcur ? a.hq1 : a.hq0)},
+                                  {(cur ? a.chunks1 : a.chunks0), (hcur ? a.hch1 : a.hch0)},
+                                  {0u, 0u},
+                                  {0u, 0u},
+                                  {lpart, kPartHeavy},
+                                  (fcur ? a.far0 : a.far1),
+                                  0u,
                                   &ctl->slot[ph % kSlots]};
             for (unsigned long long base = (unsigned long long)blockIdx.x * kBlock; base < far_len;
                  base += (unsigned long long)gridDim.x * kBlock) {
@@ -902,10 +1014,18 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
                 const bool valid = i < far_len;
                 const int v = valid ? __ldcg(&fp[i]) : 0;
                 const float d = valid ? __uint_as_float(__ldcg(&a.value[v])) : 0.0f;
-                const bool to_near = valid && d >= told && d < thr && atomicExch(&a.stamp_near[v], near_id) != near_id;
+                const bool in_bucket = valid && d >= told && d < thr;
+                int nl = 0, nh = 0;
+                if (in_bucket) {
+                    const int deg = __ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v]);
+                    nl = a.nlight ? __ldg(&a.nlight[v]) : deg;
+                    nh = deg - nl;
+                }
+                const bool light = in_bucket && nl > 0 && atomicExch(&a.stamp_near[v], near_id) != near_id;
+                const bool heavy = in_bucket && nh > 0 && atomicExch(&a.stamp_heavy[v], heavy_id) != heavy_id;
                 const bool keep = valid && d >= thr && atomicExch(&a.stamp_far[v], far_id) != far_id;
-                const unsigned deg = to_near ? (unsigned)(__ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v])) : 0u;
-                stage_push(st, to_near, v, deg);
+                stage_push(st, 0, light, v, (unsigned)nl);
+                stage_push(st, 1, heavy, v, (unsigned)nh);
                 stage_far(st, keep, v, keep ? 0x7fffffff - __float_as_int(d) : 0);
                 stage_flush(a, st, ts, out, false);
             }
@@ -917,6 +1037,9 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
             nq = s0.q_add;
             nch = s0.chunk_add;
             nbig = s0.big_add;
+            hq = s0.hq_add;
+            hch = s0.hchunk_add;
+            hbig = s0.hbig_add;
             far_len = s0.far_add;
             min_far = s0.min_far_bits;
             fcur ^= 1;
@@ -929,10 +1052,27 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
         ctl->steps = steps;
         ctl->buckets = buckets;
         ctl->bottom_up_steps = 0;
-        ctl->next_id = max(near_id, far_id) + 1;
+        ctl->next_id = max(max(near_id, far_id), heavy_id) + 2;
         *a.id_base = ctl->next_id;
     }
     write_back(a);
+}
+
+// Light-prefix length of every row for `delta` (rows are sorted by weight):
+// the first position whose weight is not below delta.
+__global__ void light_count_kernel(const int32_t *__restrict__ out_off, const float *__restrict__ out_w, int32_t V,
+                                   float delta, int32_t *__restrict__ nlight)
+{
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+        int lo = out_off[v], hi = out_off[v + 1];
+        const int rb = lo;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (out_w[mid] < delta) lo = mid + 1;
+            else hi = mid;
+        }
+        nlight[v] = lo - rb;
+    }
 }
 
 // ------------------------------------------------------------- accounting
@@ -1086,6 +1226,12 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
     }
     TRY_CUDA(cudaMalloc(&ws->stamp_near, sizeof(int32_t) * V));
     TRY_CUDA(cudaMalloc(&ws->stamp_far, sizeof(int32_t) * V));
+    TRY_CUDA(cudaMalloc(&ws->stamp_heavy, sizeof(int32_t) * V));
+    TRY_CUDA(cudaMalloc(&ws->nlight, sizeof(int32_t) * V));
+    for (int i = 0; i < 2; i++) {
+        TRY_CUDA(cudaMalloc(&ws->hq[i], sizeof(int32_t) * V));
+        TRY_CUDA(cudaMalloc(&ws->hchunks[i], sizeof(int2) * ws->chunk_cap));
+    }
     TRY_CUDA(cudaMalloc(&ws->chunks[0], sizeof(int2) * ws->chunk_cap));
     TRY_CUDA(cudaMalloc(&ws->chunks[1], sizeof(int2) * ws->chunk_cap));
     TRY_CUDA(cudaMalloc(&ws->ctl, sizeof(Ctl) * (size_t)nqueries));
@@ -1094,6 +1240,8 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
     TRY_CUDA(cudaMemsetAsync(ws->id_base, 0, sizeof(int), st));
     TRY_CUDA(cudaMemsetAsync(ws->stamp_near, 0xff, sizeof(int32_t) * V, st));
     TRY_CUDA(cudaMemsetAsync(ws->stamp_far, 0xff, sizeof(int32_t) * V, st));
+    TRY_CUDA(cudaMemsetAsync(ws->stamp_heavy, 0xff, sizeof(int32_t) * V, st));
+    ws->nlight_delta = -1.0f;
     return TRAV_OK;
 }
 
@@ -1109,6 +1257,12 @@ void workspace_free(Workspace *ws)
     }
     cudaFree(ws->stamp_near);
     cudaFree(ws->stamp_far);
+    cudaFree(ws->stamp_heavy);
+    cudaFree(ws->nlight);
+    for (int i = 0; i < 2; i++) {
+        cudaFree(ws->hq[i]);
+        cudaFree(ws->hchunks[i]);
+    }
     cudaFree(ws->chunks[0]);
     cudaFree(ws->chunks[1]);
     cudaFree(ws->ctl);
@@ -1138,6 +1292,12 @@ static TravArgs make_args(const DevGraph &g, Workspace *ws)
     a.far1 = ws->far[1];
     a.stamp_near = ws->stamp_near;
     a.stamp_far = ws->stamp_far;
+    a.stamp_heavy = ws->stamp_heavy;
+    a.hq0 = ws->hq[0];
+    a.hq1 = ws->hq[1];
+    a.hch0 = ws->hchunks[0];
+    a.hch1 = ws->hchunks[1];
+    a.nlight = nullptr;
     a.chunks = ws->chunks[0];
     a.chunks0 = ws->chunks[0];
     a.chunks1 = ws->chunks[1];
@@ -1172,6 +1332,17 @@ int launch_sssp(const DevGraph &g, Workspace *ws, int q, int32_t source_new, flo
     a.max_steps = 4 * g.V + 4096;
     a.force_dir = -1;
     a.delta = (delta > 0.0f && std::isfinite(delta)) ? delta : INFINITY;
+    if (std::isfinite(a.delta)) {
+        if (ws->nlight_delta != a.delta) {  // rows are sorted by weight: count each light prefix once per delta
+            int dev = 0, sms = 148;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            light_count_kernel<<<sms * 8, 256, 0, st>>>(g.out_off, g.out_w, g.V, a.delta, ws->nlight);
+            TRY_CUDA(cudaGetLastError());
+            ws->nlight_delta = a.delta;
+        }
+        a.nlight = ws->nlight;
+    }
     a.out = out;
     a.out_kind = out_kind;
     a.mlp = mlp;

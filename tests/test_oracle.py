@@ -137,8 +137,10 @@ def test_device_layout_restatement_is_consistent():
     want = sorted(zip(n[s], n[d], w.view(np.uint32)))
     assert got == want
     for v in range(V):
-        row = L["out_adj"][L["out_off"][v]:L["out_off"][v + 1]]
-        assert np.all(np.diff(row) >= 0)
+        row_w = L["out_w"][L["out_off"][v]:L["out_off"][v + 1]]
+        assert np.all(np.diff(row_w) >= 0)  # out rows by weight: a light prefix for any delta
+        row_in = L["in_adj"][L["in_off"][v]:L["in_off"][v + 1]]
+        assert np.all(np.diff(row_in) >= 0)
 
 
 def test_algorithmic_bytes_formulae():
