@@ -222,6 +222,19 @@ int trav_el_file_write(const char *path, int32_t directed, int32_t vertices, int
 int trav_mlp_set(trav_graph *g, int32_t kind, const float *params, int32_t count);
 int32_t trav_mlp_param_count(int32_t kind);
 
+/* Softmax cross-entropy loss of the kind's MLP on n samples (x: n x 10
+ * features, labels in [0, outputs)) and its gradient, computed on the GPU by
+ * the training kernels (forward + backward, one warp per sample).  Host
+ * buffers; grad has trav_mlp_param_count(kind) entries (may be NULL). */
+int trav_mlp_loss_grad(int32_t kind, const float *params, const float *x, const int32_t *labels, int32_t n,
+                       float *grad, float *loss);
+
+/* Train the kind's MLP in place on the GPU: `epochs` full-batch Adam steps
+ * (beta1 0.9, beta2 0.999) with learning rate lr; *final_loss (may be NULL)
+ * receives the loss after training. */
+int trav_mlp_train(int32_t kind, float *params, const float *x, const int32_t *labels, int32_t n, int32_t epochs,
+                   float lr, float *final_loss);
+
 /* ------------------------------------------------------------------- misc */
 
 const char *trav_last_error(void);

@@ -35,12 +35,20 @@ struct Slot {
     unsigned int hbig_add;        // SSSP heavy list: vertices pushed as chunk items
 };
 
+constexpr int kBarGroups = 32;    // first level of the grid barrier
+
+// One barrier arrival counter per 128-byte line (no two groups share a line).
+struct alignas(128) BarGroup {
+    unsigned int count;
+};
+
 // Control block of one persistent launch (zeroed by the host before launch).
 struct Ctl {
     unsigned int bar_count;
     unsigned int bar_gen;
     int err;
     int err_phase;
+    BarGroup bar_group[kBarGroups];
     Slot slot[kSlots];
     // written by CTA 0 as the query runs
     int steps;

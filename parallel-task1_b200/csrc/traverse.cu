@@ -53,20 +53,32 @@ __device__ __forceinline__ int ld_relaxed_int(const int *p)
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
 
-// Grid-wide barrier with a bounded wait.  Every CTA's thread 0 arrives on a
-// counter; the last one resets it and advances the generation.  Waiters give
-// up after timeout_ns (or when another CTA already failed) and the barrier
-// then returns false in every thread of the CTA.
+// Grid-wide barrier with a bounded wait.  Thread 0 of CTA b arrives on group
+// counter b % kBarGroups (one 128-byte line each, so arrivals of different
+// groups do not serialise on one address); the last arriver of a group resets
+// it and arrives on the top counter; the last top arriver resets that and
+// advances the generation, which every waiter polls.  Waiters give up after
+// timeout_ns (or when another CTA already failed) and the barrier then
+// returns false in every thread of the CTA.
 __device__ bool grid_sync(Ctl *ctl, unsigned long long timeout_ns, int phase)
 {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
+        const unsigned nb = gridDim.x;
+        const unsigned groups = nb < (unsigned)kBarGroups ? nb : (unsigned)kBarGroups;
+        const unsigned g = blockIdx.x % groups;
+        const unsigned in_group = (nb - g + groups - 1) / groups;  // CTAs b < nb with b % groups == g
         unsigned gen = ld_acquire(&ctl->bar_gen);
         __threadfence();
-        unsigned arrived = atomicAdd(&ctl->bar_count, 1u);
-        if (arrived == gridDim.x - 1) {
+        bool last = false;
+        if (atomicAdd(&ctl->bar_group[g].count, 1u) == in_group - 1) {
+            atomicExch(&ctl->bar_group[g].count, 0u);
+            __threadfence();  // order the group's arrivals before the top arrival
+            last = atomicAdd(&ctl->bar_count, 1u) == groups - 1;
+        }
+        if (last) {
             atomicExch(&ctl->bar_count, 0u);
             __threadfence();
             atomicAdd(&ctl->bar_gen, 1u);
@@ -775,15 +787,47 @@ __global__ void __launch_bounds__(kBlock) bfs_persistent(TravArgs a)
             for (unsigned w0 = blockIdx.x * kWarps; w0 < (unsigned)a.W; w0 += gridDim.x * kWarps) {
                 const unsigned w = w0 + wic;
                 if (w < (unsigned)a.W) {
-                    const int v = (int)(w * 32 + lane_id());
-                    const unsigned vis = __ldcg(&a.visited[w]);
+                    // The frontier bitmap and this word of `visited` were written in
+                    // earlier phases and only this warp writes the word now: plain
+                    // (L1-cacheable) loads are coherent after the grid barrier.
+                    const int lane = (int)lane_id();
+                    const int v = (int)(w * 32 + lane);
+                    const unsigned vis = a.visited[w];
+                    bool cand = v < a.V && !((vis >> lane) & 1u);
+                    int k = 0, kend = 0;
+                    if (cand) {
+                        k = __ldg(&a.in_off[v]);
+                        kend = __ldg(&a.in_off[v + 1]);
+                    }
                     bool found = false;
-                    if (v < a.V && !((vis >> lane_id()) & 1u)) {
-                        int k = __ldg(&a.in_off[v]);
-                        const int kend = __ldg(&a.in_off[v + 1]);
+                    // long in-rows: the whole warp scans one row 32 entries at a time
+                    unsigned coop = __ballot_sync(kFull, cand && kend - k > 32);
+                    while (coop) {
+                        const int owner = __ffs(coop) - 1;
+                        coop &= coop - 1;
+                        const int kb = __shfl_sync(kFull, k, owner), ke = __shfl_sync(kFull, kend, owner);
+                        bool hit = false;
+                        for (int kk = kb + lane; kk - lane < ke; kk += 32) {
+                            bool h = false;
+                            if (kk < ke) {
+                                const int u = __ldg(&a.in_adj[kk]);
+                                h = (fc[u >> 5] >> (u & 31)) & 1u;
+                            }
+                            if (__any_sync(kFull, h)) {
+                                hit = true;
+                                break;
+                            }
+                        }
+                        if (lane == owner) {
+                            found = hit;
+                            cand = false;
+                        }
+                    }
+                    // short in-rows: one lane each
+                    if (cand) {
                         for (; k < kend; k++) {
                             const int u = __ldg(&a.in_adj[k]);
-                            if ((__ldcg(&fc[u >> 5]) >> (u & 31)) & 1u) { found = true; break; }
+                            if ((fc[u >> 5] >> (u & 31)) & 1u) { found = true; break; }
                         }
                     }
                     const unsigned m = __ballot_sync(kFull, found);

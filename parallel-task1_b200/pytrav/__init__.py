@@ -46,7 +46,7 @@ EXPORTS = [
     "trav_bfs", "trav_sssp", "trav_last_stats", "trav_last_bfs_trace", "trav_init_distances_f32",
     "trav_bellman_ford_el_f32", "trav_bfs_el", "trav_el_file_read", "trav_el_file_write", "trav_mlp_set",
     "trav_mlp_param_count", "trav_last_error", "trav_version", "trav_last_batch_ms", "trav_graph_set_stream",
-    "trav_bfs_csr_noalloc", "trav_last_phase_log",
+    "trav_bfs_csr_noalloc", "trav_last_phase_log", "trav_mlp_loss_grad", "trav_mlp_train",
 ]
 
 
@@ -103,6 +103,8 @@ def lib():
         L.trav_graph_set_stream.argtypes = [vp, vp]
         L.trav_bfs_csr_noalloc.argtypes = [vp, vp, i32, i64, i32, vp, vp]
         L.trav_last_phase_log.argtypes = [vp, vp, vp, vp, vp, i32, C.POINTER(i32)]
+        L.trav_mlp_loss_grad.argtypes = [i32, vp, vp, vp, i32, vp, C.POINTER(f32)]
+        L.trav_mlp_train.argtypes = [i32, vp, vp, vp, i32, i32, f32, C.POINTER(f32)]
         _lib = L
     return _lib
 
@@ -278,6 +280,43 @@ class Graph:
 
 def mlp_param_count(kind: int) -> int:
     return int(lib().trav_mlp_param_count(kind))
+
+
+MLP_FEATURES = 10
+
+
+def mlp_loss_grad(kind: int, params, x, labels):
+    """(loss, gradient) of the schedule MLP on the GPU training kernels."""
+    p = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(x, np.float32).reshape(-1, MLP_FEATURES)
+    y = np.ascontiguousarray(labels, np.int32)
+    g = np.empty_like(p)
+    loss = C.c_float()
+    _check(lib().trav_mlp_loss_grad(kind, p.ctypes.data, x.ctypes.data, y.ctypes.data, len(y), g.ctypes.data,
+                                    C.byref(loss)))
+    return float(loss.value), g
+
+
+def mlp_train(kind: int, params, x, labels, epochs: int = 500, lr: float = 1e-2):
+    """Train in place with full-batch Adam on the GPU; returns (params, final loss)."""
+    p = np.array(params, np.float32)
+    x = np.ascontiguousarray(x, np.float32).reshape(-1, MLP_FEATURES)
+    y = np.ascontiguousarray(labels, np.int32)
+    loss = C.c_float()
+    _check(lib().trav_mlp_train(kind, p.ctypes.data, x.ctypes.data, y.ctypes.data, len(y), epochs, lr, C.byref(loss)))
+    return p, float(loss.value)
+
+
+def mlp_init(kind: int, seed: int = 0):
+    """Glorot-uniform weights, zero biases, in the packed layout."""
+    rng = np.random.default_rng(seed)
+    F, H, O = MLP_FEATURES, 32, (2 if kind == 0 else 4)
+    parts = []
+    for fan_in, fan_out in ((F, H), (H, H), (H, O)):
+        lim = np.sqrt(6.0 / (fan_in + fan_out))
+        parts.append(rng.uniform(-lim, lim, fan_in * fan_out))
+        parts.append(np.zeros(fan_out))
+    return np.concatenate(parts).astype(np.float32)
 
 
 # ----------------------------------------------- reference-shaped wrappers
