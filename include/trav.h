@@ -235,6 +235,21 @@ int trav_mlp_loss_grad(int32_t kind, const float *params, const float *x, const 
 int trav_mlp_train(int32_t kind, float *params, const float *x, const int32_t *labels, int32_t n, int32_t epochs,
                    float lr, float *final_loss);
 
+/* Force the schedule's decisions for the following queries of one kind on
+ * this handle (used to time alternatives when building training traces):
+ * decision i takes option plan[i] when plan[i] < 255 and follows the schedule
+ * otherwise.  BFS decision i is the direction of step i (0 top-down, 1
+ * bottom-up); SSSP decision i is the width option of the i-th bucket opening
+ * (delta x 1, 2, 4, 8).  n == 0 clears the plan. */
+int trav_set_plan(trav_graph *g, int32_t kind, const uint8_t *plan, int32_t n);
+
+/* Decisions of the last query (the last source of a batch): per decision the
+ * 10 MLP input features (x[i*10 + k]), the option taken, the index of the
+ * phase it opened (see trav_last_phase_log) and, for SSSP, the new bucket
+ * [lo, hi).  Up to cap entries (any array may be NULL); *n receives the count. */
+int trav_last_decisions(trav_graph *g, float *x, uint8_t *choice, int32_t *phase, float *lo, float *hi, int32_t cap,
+                        int32_t *n);
+
 /* ------------------------------------------------------------------- misc */
 
 const char *trav_last_error(void);

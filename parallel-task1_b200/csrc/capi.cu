@@ -404,6 +404,45 @@ int trav_graph_set_stream(trav_graph *g, void *stream)
     return TRAV_OK;
 }
 
+int trav_set_plan(trav_graph *g, int32_t kind, const uint8_t *plan, int32_t n)
+{
+    if (!g) return bad("graph handle is NULL");
+    if (kind != 0 && kind != 1) return bad("kind must be 0 (BFS) or 1 (SSSP)");
+    if (n < 0 || (n > 0 && !plan)) return bad("plan must hold n >= 0 entries");
+    TRY_CUDA(cudaSetDevice(g->device));
+    TRY_CUDA(cudaStreamSynchronize(g->st));
+    cudaFree(g->ws.plan[kind]);
+    g->ws.plan[kind] = nullptr;
+    g->ws.plan_len[kind] = 0;
+    if (n == 0) return TRAV_OK;
+    TRY_CUDA(cudaMalloc(&g->ws.plan[kind], (size_t)n));
+    TRY_CUDA(cudaMemcpy(g->ws.plan[kind], plan, (size_t)n, cudaMemcpyHostToDevice));
+    g->ws.plan_len[kind] = n;
+    return TRAV_OK;
+}
+
+int trav_last_decisions(trav_graph *g, float *x, uint8_t *choice, int32_t *phase, float *lo, float *hi, int32_t cap,
+                        int32_t *n)
+{
+    if (!g || !n) return bad("graph handle and n must not be NULL");
+    if (g->last_n < 1) return bad("no query has run on this handle");
+    TRY_CUDA(cudaSetDevice(g->device));
+    std::unique_ptr<Ctl> h(new Ctl);
+    TRY_CUDA(cudaMemcpy(h.get(), g->ws.ctl + (g->last_n - 1), sizeof(Ctl), cudaMemcpyDeviceToHost));
+    *n = h->ndec;
+    int m = h->ndec < cap ? h->ndec : cap;
+    if (m > kMaxDec) m = kMaxDec;
+    for (int i = 0; i < m; i++) {
+        if (x)
+            for (int k = 0; k < kDecFeat; k++) x[i * kDecFeat + k] = h->dec_x[i][k];
+        if (choice) choice[i] = h->dec_choice[i];
+        if (phase) phase[i] = h->dec_phase[i];
+        if (lo) lo[i] = h->dec_lo[i];
+        if (hi) hi[i] = h->dec_hi[i];
+    }
+    return TRAV_OK;
+}
+
 int trav_last_phase_log(trav_graph *g, uint8_t *kind, int64_t *size, double *end_us, int64_t *edges, int32_t cap,
                         int32_t *n)
 {

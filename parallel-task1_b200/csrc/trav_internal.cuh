@@ -16,6 +16,8 @@ constexpr int kBigDegree = 512;   // rows longer than this are split into chunks
 constexpr int kSmallDeg = 32;     // one-phase expansion: rows up to this length go to the CTA-tile queue
 constexpr int kItem = 256;        // one-phase expansion: edges per chunk item of a longer row
 constexpr int kMaxTrace = 4096;   // steps recorded per query
+constexpr int kMaxDec = 1024;     // schedule decisions recorded per query
+constexpr int kDecFeat = 10;      // features per decision (the schedule MLP's input width)
 constexpr int kSlots = 4;         // ring of per-phase counter slots
 
 // Device status codes written to Ctl::err.
@@ -67,6 +69,13 @@ struct Ctl {
     unsigned long long ph_end_ns[kMaxTrace];
     unsigned long long ph_scanned[kMaxTrace];
     unsigned long long t0_ns;     // %globaltimer after initialisation
+    // schedule decisions (CTA 0): the MLP features, the choice taken, the
+    // phase index the decision opened, and for SSSP the new bucket [lo, hi)
+    int ndec;
+    float dec_x[kMaxDec][kDecFeat];
+    unsigned char dec_choice[kMaxDec];
+    int dec_phase[kMaxDec];
+    float dec_lo[kMaxDec], dec_hi[kMaxDec];
 };
 
 // Device graph: int32 CSR over relabelled ids + transposed CSR.
@@ -103,6 +112,8 @@ struct Workspace {
     Ctl *ctl = nullptr;                // ctl_cap control blocks: one per query of a batch
     int ctl_cap = 0;
     int *id_base = nullptr;            // device: first unused stamp id (continues across queries)
+    unsigned char *plan[2] = {nullptr, nullptr};  // forced decisions for BFS / SSSP queries (device)
+    int plan_len[2] = {0, 0};
 };
 
 // Arguments of the persistent kernels (passed by value).
@@ -144,6 +155,9 @@ struct TravArgs {
     int32_t out_kind;      // 0 = int32 levels, 1 = float distances, 2 = uint8 reached flags
     // learned schedule (nullptr = plain)
     const float *mlp;
+    // forced decisions: plan[i] (< 255) overrides decision i of the query
+    const unsigned char *plan;
+    int32_t plan_len;
     unsigned long long timeout_ns;
 };
 

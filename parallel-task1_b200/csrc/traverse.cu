@@ -147,6 +147,29 @@ __device__ __forceinline__ void clear_ahead(Ctl *ctl, int ph)
     }
 }
 
+// Decision log entry (CTA 0 thread 0).  Returns the plan's override of
+// decision `i` or -1.
+__device__ __forceinline__ int planned(const TravArgs &a, int i)
+{
+    return (a.plan && i < a.plan_len && a.plan[i] != 255) ? (int)a.plan[i] : -1;
+}
+
+__device__ __forceinline__ void log_decision(Ctl *ctl, const Feat &f, int choice, float lo, float hi)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const int i = ctl->ndec;
+        if (i < kMaxDec) {
+#pragma unroll
+            for (int k = 0; k < kDecFeat; k++) ctl->dec_x[i][k] = f.x[k];
+            ctl->dec_choice[i] = (unsigned char)choice;
+            ctl->dec_phase[i] = ctl->nphase;
+            ctl->dec_lo[i] = lo;
+            ctl->dec_hi[i] = hi;
+        }
+        ctl->ndec = i + 1;
+    }
+}
+
 // Phase log entry, written by CTA 0 thread 0 right after a grid barrier.
 __device__ __forceinline__ void log_phase(Ctl *ctl, int kind, unsigned size)
 {
@@ -748,11 +771,15 @@ __global__ void __launch_bounds__(kBlock) bfs_persistent(TravArgs a)
         }
         // direction for this step (same inputs in every CTA -> same answer)
         if (threadIdx.x < 32) {
+            const Feat f = bfs_features(L, nf, mf, mu, nf_prev, a.V, a.E, prev_dir);
             int d = dir;
             if (a.force_dir >= 0) d = (L == 0) ? 0 : a.force_dir;
-            else if (a.mlp) d = mlp_argmax_warp(a.mlp, bfs_features(L, nf, mf, mu, nf_prev, a.V, a.E, prev_dir), kBfsOut);
+            else if (a.mlp) d = mlp_argmax_warp(a.mlp, f, kBfsOut);
             else if (dir == 0) { if ((double)mf > (double)mu / a.alpha) d = 1; }
             else if (!(nf >= nf_prev || (double)nf > (double)a.V / a.beta)) d = 0;
+            const int forced = planned(a, L);
+            if (forced >= 0) d = forced;
+            log_decision(ctl, f, d, 0.0f, 0.0f);
             if (threadIdx.x == 0) s_dir = d;
         }
         __syncthreads();
@@ -1028,18 +1055,20 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
         } else if (far_len > 0) {
             // open the next bucket (skipping empty ones): bound = max(old, min far) + width
             if (threadIdx.x < 32) {
-                float d = a.delta;
-                if (a.mlp)
-                    d = a.delta * sssp_width_scale(mlp_argmax_warp(
-                                      a.mlp, sssp_features(steps, far_len, __int_as_float(min_far), thr, a.delta, a.V, a.E, buckets),
-                                      kSsspOut));
-                if (threadIdx.x == 0) s_delta = d;
+                const Feat f = sssp_features(steps, far_len, __int_as_float(min_far), thr, a.delta, a.V, a.E, buckets);
+                int o = 0;
+                if (a.mlp) o = mlp_argmax_warp(a.mlp, f, kSsspOut);
+                const int forced = planned(a, buckets - 1);
+                if (forced >= 0) o = forced;
+                const float width = a.delta * sssp_width_scale(o);
+                float hi = __fadd_rn(fmaxf(thr, __int_as_float(min_far)), width);
+                if (!(hi > thr)) hi = nextafterf(thr, INFINITY);
+                log_decision(ctl, f, o, thr, hi);
+                if (threadIdx.x == 0) s_delta = hi;
             }
             __syncthreads();
-            const float width = s_delta;
             const float told = thr;
-            thr = __fadd_rn(fmaxf(told, __int_as_float(min_far)), width);
-            if (!(thr > told)) thr = nextafterf(told, INFINITY);
+            thr = s_delta;  // the new bound, computed once above (same inputs in every CTA)
             far_id++;
             const int32_t *fp = fcur ? a.far1 : a.far0;
             clear_ahead(ctl, ph);
@@ -1311,6 +1340,8 @@ void workspace_free(Workspace *ws)
     cudaFree(ws->chunks[1]);
     cudaFree(ws->ctl);
     cudaFree(ws->id_base);
+    cudaFree(ws->plan[0]);
+    cudaFree(ws->plan[1]);
     *ws = Workspace{};
 }
 
@@ -1364,6 +1395,8 @@ int launch_bfs(const DevGraph &g, Workspace *ws, int q, int32_t source_new, cons
     a.out = out;
     a.out_kind = out_kind;
     a.mlp = mlp;
+    a.plan = ws->plan[0];
+    a.plan_len = ws->plan_len[0];
     return enqueue_persistent(0, a, st, ev0, ev1);
 }
 
@@ -1390,6 +1423,8 @@ int launch_sssp(const DevGraph &g, Workspace *ws, int q, int32_t source_new, flo
     a.out = out;
     a.out_kind = out_kind;
     a.mlp = mlp;
+    a.plan = ws->plan[1];
+    a.plan_len = ws->plan_len[1];
     return enqueue_persistent(1, a, st, ev0, ev1);
 }
 

@@ -46,7 +46,8 @@ EXPORTS = [
     "trav_bfs", "trav_sssp", "trav_last_stats", "trav_last_bfs_trace", "trav_init_distances_f32",
     "trav_bellman_ford_el_f32", "trav_bfs_el", "trav_el_file_read", "trav_el_file_write", "trav_mlp_set",
     "trav_mlp_param_count", "trav_last_error", "trav_version", "trav_last_batch_ms", "trav_graph_set_stream",
-    "trav_bfs_csr_noalloc", "trav_last_phase_log", "trav_mlp_loss_grad", "trav_mlp_train",
+    "trav_bfs_csr_noalloc", "trav_last_phase_log", "trav_mlp_loss_grad", "trav_mlp_train", "trav_set_plan",
+    "trav_last_decisions",
 ]
 
 
@@ -105,6 +106,8 @@ def lib():
         L.trav_last_phase_log.argtypes = [vp, vp, vp, vp, vp, i32, C.POINTER(i32)]
         L.trav_mlp_loss_grad.argtypes = [i32, vp, vp, vp, i32, vp, C.POINTER(f32)]
         L.trav_mlp_train.argtypes = [i32, vp, vp, vp, i32, i32, f32, C.POINTER(f32)]
+        L.trav_set_plan.argtypes = [vp, i32, vp, i32]
+        L.trav_last_decisions.argtypes = [vp, vp, vp, vp, vp, vp, i32, C.POINTER(i32)]
         _lib = L
     return _lib
 
@@ -252,6 +255,25 @@ class Graph:
                                          edges.ctypes.data, cap, C.byref(n)))
         k = min(n.value, cap)
         return kind[:k].copy(), size[:k].copy(), end[:k].copy(), edges[:k].copy()
+
+    def set_plan(self, kind: int, plan=None):
+        """Force decisions of later queries of `kind` (0 BFS, 1 SSSP); entries of 255 follow the schedule."""
+        p = np.ascontiguousarray(plan if plan is not None else [], np.uint8)
+        _check(lib().trav_set_plan(self._h, kind, p.ctypes.data if len(p) else None, len(p)))
+
+    def last_decisions(self):
+        """Decisions of the last query: (features [n,10], choice, phase index, lo, hi)."""
+        cap = 1024
+        x = np.zeros((cap, 10), np.float32)
+        ch = np.zeros(cap, np.uint8)
+        ph = np.zeros(cap, np.int32)
+        lo = np.zeros(cap, np.float32)
+        hi = np.zeros(cap, np.float32)
+        n = C.c_int32()
+        _check(lib().trav_last_decisions(self._h, x.ctypes.data, ch.ctypes.data, ph.ctypes.data, lo.ctypes.data,
+                                         hi.ctypes.data, cap, C.byref(n)))
+        k = min(n.value, cap)
+        return x[:k].copy(), ch[:k].copy(), ph[:k].copy(), lo[:k].copy(), hi[:k].copy()
 
     def set_mlp(self, kind: int, params):
         p = np.ascontiguousarray(params, np.float32)
