@@ -215,7 +215,7 @@ int trav_el_file_write(const char *path, int32_t directed, int32_t vertices, int
 
 /* Install the parameters of a schedule MLP on a handle (copied to the
  * device).  kind 0 = BFS direction (2 outputs: top-down, bottom-up);
- * kind 1 = SSSP bucket width (4 outputs: delta x 1, 2, 4, 8).  count must be
+ * kind 1 = SSSP bucket width (4 outputs: delta x 1, 4, 16, 64).  count must be
  * trav_mlp_param_count(kind).  Layout: [W1 (32x10) | b1 (32) | W2 (32x32) |
  * b2 (32) | W3 (Ox32) | b3 (O)], row-major, tanh hidden units.  New; the
  * reference has no learned schedule. */
@@ -240,7 +240,7 @@ int trav_mlp_train(int32_t kind, float *params, const float *x, const int32_t *l
  * decision i takes option plan[i] when plan[i] < 255 and follows the schedule
  * otherwise.  BFS decision i is the direction of step i (0 top-down, 1
  * bottom-up); SSSP decision i is the width option of the i-th bucket opening
- * (delta x 1, 2, 4, 8).  n == 0 clears the plan. */
+ * (delta x 1, 4, 16, 64).  n == 0 clears the plan. */
 int trav_set_plan(trav_graph *g, int32_t kind, const uint8_t *plan, int32_t n);
 
 /* Decisions of the last query (the last source of a batch): per decision the

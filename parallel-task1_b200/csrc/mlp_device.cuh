@@ -16,7 +16,7 @@ namespace trav {
 constexpr int kFeat = 10;
 constexpr int kHidden = 32;
 constexpr int kBfsOut = 2;      // 0 = top-down (push), 1 = bottom-up (pull)
-constexpr int kSsspOut = 4;     // bucket width = delta * {1, 2, 4, 8} (merge 1, 2, 4, 8 buckets)
+constexpr int kSsspOut = 4;     // bucket width = delta * {1, 4, 16, 64} (merge 1, 4, 16, 64 buckets)
 
 __host__ __device__ constexpr int mlp_param_count(int O)
 {
@@ -70,7 +70,7 @@ __host__ __device__ inline Feat sssp_features(int steps, unsigned long long far_
     return f;
 }
 
-__host__ __device__ inline float sssp_width_scale(int option) { return (float)(1 << option); }
+__host__ __device__ inline float sssp_width_scale(int option) { return (float)(1 << (2 * option)); }
 
 #ifdef __CUDACC__
 // Warp-cooperative forward pass: lane j owns hidden unit j.  All 32 lanes

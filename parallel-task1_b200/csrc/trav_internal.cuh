@@ -59,6 +59,7 @@ struct Ctl {
     int next_id;                  // first unused stamp id after the query
     unsigned long long edges_scanned;  // out-edges expanded (push-side work, all steps)
     int nphase;                   // phases logged below
+    int ndec;                     // schedule decisions logged below
     unsigned char dirs[kMaxTrace];       // BFS: direction of step s (0 top-down, 1 bottom-up)
     unsigned int frontier[kMaxTrace];    // BFS: frontier size of step s; SSSP: of expansion s
     // phase log (CTA 0, after each grid barrier): kind (0 top-down, 1 bottom-up,
@@ -71,7 +72,6 @@ struct Ctl {
     unsigned long long t0_ns;     // %globaltimer after initialisation
     // schedule decisions (CTA 0): the MLP features, the choice taken, the
     // phase index the decision opened, and for SSSP the new bucket [lo, hi)
-    int ndec;
     float dec_x[kMaxDec][kDecFeat];
     unsigned char dec_choice[kMaxDec];
     int dec_phase[kMaxDec];

@@ -355,37 +355,41 @@ __device__ void write_back(const TravArgs &a)
 // ------------------------------------------------------ one-phase frontier
 // The next frontier is written in two parts while it is discovered: vertices
 // whose row to expand has at most kSmallDeg edges go to a queue that the next
-// step expands by CTA tiles; longer rows are cut into kItem-edge items,
-// expanded one warp per item.  Both parts are complete when the step's
-// barrier passes, so a step is one phase and one grid barrier, and the work
-// of long rows is spread over every warp of the grid.
+// step expands in 32-vertex warp tiles; longer rows are cut into kItem-edge
+// items, expanded one warp per item.  Both parts are complete when the step's
+// barrier passes, so a step is one phase and one grid barrier, and the work of
+// long rows is spread over every warp of the grid.
 //
-// Pushes are staged per CTA in shared memory and written out in bulk: one
-// global atomic reserves room for up to a thousand or more entries, and the
-// scalar counters (out-degree sums, scanned edges, far minimum) are reduced
-// per CTA per phase.  Without this every warp hit the same few counters and
-// serialised on one L2 slice.  All loops that push are CTA-uniform, so the
-// flush points can use __syncthreads.
+// Expansion is warp-centric: no CTA barrier inside a phase.  Every warp stages
+// its pushes in its own shared-memory buffers and writes them out in bulk (one
+// global atomic reserves room for up to a few hundred entries); the scalar
+// counters are kept per warp and reduced per CTA once at the end of the phase.
 //
 // A push goes to one of two targets: target 0 is the next frontier (for SSSP
 // its rows are the light prefixes, w < delta), target 1 is the SSSP heavy list
 // (rows are the heavy suffixes).  Rows are sorted by weight, so both parts are
 // contiguous: [off[v], off[v] + nlight[v]) and [off[v] + nlight[v], off[v+1]).
-constexpr int kBatch = 4;                      // independent edges per lane per round
-constexpr int kRoundPush = kBlock * kBatch;    // most pushes a CTA makes between two flush points
-constexpr int kFlushQ = 1024, kFlushBig = 128, kFlushFar = 1024;
+constexpr int kBatch = 4;  // independent edges per lane per round
+// Per-warp buffers: a push adds at most 32 entries to a buffer that held
+// fewer than its flush mark, so mark + 32 entries always fit.
+constexpr int kWQFlush = 128, kWQ = kWQFlush + 32;
+constexpr int kWBigFlush = 64, kWBig = kWBigFlush + 32;
+constexpr int kWFarFlush = 128, kWFar = kWFarFlush + 32;
 
 constexpr int kPartWhole = 0, kPartLight = 1, kPartHeavy = 2;
 
-struct Stage {
-    int q[2][kFlushQ + kRoundPush];
-    int big[2][kFlushBig + kRoundPush];
-    int far[kFlushFar + kRoundPush];
-    unsigned nq[2], nbig[2], nfar;
-    unsigned base_q[2], base_far, base_items;
+struct WarpStage {
+    int q[2][kWQ];
+    int big[2][kWBig];
+    int far[kWFar];
+    int tu[32], trb[32], tpre[32];  // the current warp tile
+    float tdu[32];
+};
+
+struct CtaCounters {
+    unsigned long long mf, scanned;
     unsigned big_total[2];
     int far_key;
-    unsigned long long mf, scanned;
 };
 
 // Destination of one phase's pushes.
@@ -400,6 +404,17 @@ struct FrontierOut {
     Slot *slot;
 };
 
+// Per-warp push state (counts are warp-uniform registers).
+struct Pusher {
+    const TravArgs *a;
+    const FrontierOut *o;
+    WarpStage *s;
+    unsigned nq[2], nbig[2], nfar;
+    unsigned big_total[2];
+    unsigned long long mf, scanned;  // lane-partial sums
+    int far_key;                     // lane-partial max
+};
+
 // Row part [begin, end) of vertex v.
 __device__ __forceinline__ int2 row_part(const TravArgs &a, int v, int part)
 {
@@ -409,207 +424,218 @@ __device__ __forceinline__ int2 row_part(const TravArgs &a, int v, int part)
     return make_int2(rb, re);
 }
 
-__device__ __forceinline__ void stage_init(Stage &st)
+__device__ __forceinline__ Pusher make_pusher(const TravArgs &a, const FrontierOut &o, WarpStage *s)
 {
-    if (threadIdx.x == 0) {
-        st.nq[0] = st.nq[1] = st.nbig[0] = st.nbig[1] = st.nfar = 0;
-        st.big_total[0] = st.big_total[1] = 0;
-        st.far_key = 0;
-        st.mf = st.scanned = 0;
+    Pusher p;
+    p.a = &a;
+    p.o = &o;
+    p.s = s;
+    p.nq[0] = p.nq[1] = p.nbig[0] = p.nbig[1] = p.nfar = 0;
+    p.big_total[0] = p.big_total[1] = 0;
+    p.mf = p.scanned = 0;
+    p.far_key = 0;
+    return p;
+}
+
+__device__ __forceinline__ void flush_q(Pusher &p, int t)
+{
+    __syncwarp();
+    unsigned base = 0;
+    if (lane_id() == 0) base = p.o->qbase[t] + atomicAdd(t ? &p.o->slot->hq_add : &p.o->slot->q_add, p.nq[t]);
+    base = __shfl_sync(kFull, base, 0);
+    for (unsigned i = lane_id(); i < p.nq[t]; i += 32) p.o->q[t][base + i] = p.s->q[t][i];
+    __syncwarp();
+    p.nq[t] = 0;
+}
+
+__device__ __forceinline__ void flush_big(Pusher &p, int t)
+{
+    __syncwarp();
+    for (unsigned r = 0; r < p.nbig[t]; r += 32) {
+        const unsigned i = r + lane_id();
+        int v = 0, nch = 0;
+        int2 part = make_int2(0, 0);
+        if (i < p.nbig[t]) {
+            v = p.s->big[t][i];
+            part = row_part(*p.a, v, p.o->part[t]);
+            nch = (part.y - part.x + kItem - 1) / kItem;
+        }
+        int incl = nch;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int y = __shfl_up_sync(kFull, incl, d);
+            if ((int)lane_id() >= d) incl += y;
+        }
+        const unsigned total = (unsigned)__shfl_sync(kFull, incl, 31);
+        unsigned base = 0;
+        if (lane_id() == 0) base = p.o->cbase[t] + atomicAdd(t ? &p.o->slot->hchunk_add : &p.o->slot->chunk_add, total);
+        base = __shfl_sync(kFull, base, 0) + (unsigned)(incl - nch);
+        for (int c = 0; c < nch; c++) p.o->chunks[t][base + c] = make_int2(v, part.x + c * kItem);
     }
-    __syncthreads();
+    __syncwarp();
+    p.nbig[t] = 0;
+}
+
+__device__ __forceinline__ void flush_far(Pusher &p)
+{
+    __syncwarp();
+    unsigned base = 0;
+    if (lane_id() == 0) base = p.o->fbase + atomicAdd(&p.o->slot->far_add, p.nfar);
+    base = __shfl_sync(kFull, base, 0);
+    for (unsigned i = lane_id(); i < p.nfar; i += 32) p.o->farp[base + i] = p.s->far[i];
+    __syncwarp();
+    p.nfar = 0;
 }
 
 // Warp-collective: lanes with `flag` push vertex v to target t; `len` is the
 // length of the row part the target will expand (tile queue or chunk items).
-__device__ __forceinline__ void stage_push(Stage &st, int t, bool flag, int v, unsigned len)
+__device__ __forceinline__ void push(Pusher &p, int t, bool flag, int v, unsigned len)
 {
     const bool big = flag && len > (unsigned)kSmallDeg;
     const bool small = flag && !big;
     const unsigned ms = __ballot_sync(kFull, small), mb = __ballot_sync(kFull, big);
     if (ms) {
-        const unsigned leader = __ffs(ms) - 1;
-        unsigned pos = 0;
-        if (lane_id() == leader) pos = atomicAdd(&st.nq[t], (unsigned)__popc(ms));
-        pos = __shfl_sync(kFull, pos, leader);
-        if (small) st.q[t][pos + __popc(ms & lanemask_lt())] = v;
+        if (small) p.s->q[t][p.nq[t] + __popc(ms & lanemask_lt())] = v;
+        p.nq[t] += __popc(ms);
+        if (p.nq[t] >= (unsigned)kWQFlush) flush_q(p, t);
     }
     if (mb) {
-        const unsigned leader = __ffs(mb) - 1;
-        unsigned pos = 0;
-        if (lane_id() == leader) {
-            pos = atomicAdd(&st.nbig[t], (unsigned)__popc(mb));
-            atomicAdd(&st.big_total[t], (unsigned)__popc(mb));
-        }
-        pos = __shfl_sync(kFull, pos, leader);
-        if (big) st.big[t][pos + __popc(mb & lanemask_lt())] = v;
+        if (big) p.s->big[t][p.nbig[t] + __popc(mb & lanemask_lt())] = v;
+        p.nbig[t] += __popc(mb);
+        p.big_total[t] += __popc(mb);
+        if (p.nbig[t] >= (unsigned)kWBigFlush) flush_big(p, t);
     }
 }
 
 // Warp-collective: lanes with `flag` add v to the far pile; key = 0x7fffffff - distance bits.
-__device__ __forceinline__ void stage_far(Stage &st, bool flag, int v, int key)
+__device__ __forceinline__ void push_far(Pusher &p, bool flag, int v, int key)
 {
     const unsigned m = __ballot_sync(kFull, flag);
     if (!m) return;
-    const unsigned leader = __ffs(m) - 1;
-    unsigned pos = 0;
-    if (lane_id() == leader) pos = atomicAdd(&st.nfar, (unsigned)__popc(m));
-    pos = __shfl_sync(kFull, pos, leader);
-    if (flag) st.far[pos + __popc(m & lanemask_lt())] = v;
-    key = __reduce_max_sync(kFull, flag ? key : 0);
-    if (lane_id() == 0) atomicMax(&st.far_key, key);
+    if (flag) {
+        p.s->far[p.nfar + __popc(m & lanemask_lt())] = v;
+        p.far_key = max(p.far_key, key);
+    }
+    p.nfar += __popc(m);
+    if (p.nfar >= (unsigned)kWFarFlush) flush_far(p);
 }
 
-__device__ __forceinline__ void stage_add_mf(Stage &st, unsigned x)
+// End of a phase: every warp writes out what it staged, then the CTA reduces
+// the counters and publishes them with one atomic each.  CTA-collective.
+__device__ void finish_phase(Pusher &p, CtaCounters &cc)
 {
-    const unsigned s = __reduce_add_sync(kFull, x);
-    if (s && lane_id() == 0) atomicAdd(&st.mf, (unsigned long long)s);
-}
-
-// CTA-collective: write staged entries out when a buffer passed its flush
-// mark (or all of them when `final`, which also publishes the counters).
-// Between two calls a CTA pushes at most kRoundPush entries per buffer.
-__device__ void stage_flush(const TravArgs &a, Stage &st, TileShared &ts, const FrontierOut &o, bool final)
-{
-    __syncthreads();
     for (int t = 0; t < 2; t++) {
-        const unsigned nq = st.nq[t], nbig = st.nbig[t];
-        const bool dq = nq > 0 && (final || nq >= (unsigned)kFlushQ);
-        const bool db = nbig > 0 && (final || nbig >= (unsigned)kFlushBig);
-        if (!(dq || db)) continue;
-        if (dq && threadIdx.x == 0) st.base_q[t] = o.qbase[t] + atomicAdd(t ? &o.slot->hq_add : &o.slot->q_add, nq);
-        if (db) {
-            for (unsigned r = 0; r < nbig; r += kBlock) {
-                const unsigned i = r + threadIdx.x;
-                int v = 0, nch = 0;
-                int2 p = make_int2(0, 0);
-                if (i < nbig) {
-                    v = st.big[t][i];
-                    p = row_part(a, v, o.part[t]);
-                    nch = (p.y - p.x + kItem - 1) / kItem;
-                }
-                const int pre = block_excl_scan(nch, ts);
-                if (threadIdx.x == 0)
-                    st.base_items = o.cbase[t] + atomicAdd(t ? &o.slot->hchunk_add : &o.slot->chunk_add, (unsigned)ts.total);
-                __syncthreads();
-                const unsigned base = st.base_items + (unsigned)pre;
-                for (int c = 0; c < nch; c++) o.chunks[t][base + c] = make_int2(v, p.x + c * kItem);
-                __syncthreads();
-            }
-        }
-        __syncthreads();
-        if (dq)
-            for (unsigned i = threadIdx.x; i < nq; i += kBlock) o.q[t][st.base_q[t] + i] = st.q[t][i];
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            if (dq) st.nq[t] = 0;
-            if (db) st.nbig[t] = 0;
-        }
+        if (p.nq[t]) flush_q(p, t);
+        if (p.nbig[t]) flush_big(p, t);
     }
-    const unsigned nfar = st.nfar;
-    if (nfar > 0 && (final || nfar >= (unsigned)kFlushFar)) {
-        if (threadIdx.x == 0) st.base_far = o.fbase + atomicAdd(&o.slot->far_add, nfar);
-        __syncthreads();
-        for (unsigned i = threadIdx.x; i < nfar; i += kBlock) o.farp[st.base_far + i] = st.far[i];
-        __syncthreads();
-        if (threadIdx.x == 0) st.nfar = 0;
-    }
-    if (final && threadIdx.x == 0) {
-        if (st.mf) atomicAdd(&o.slot->mf, st.mf);
-        if (st.scanned) atomicAdd(&a.ctl->edges_scanned, st.scanned);
-        if (st.big_total[0]) atomicAdd(&o.slot->big_add, st.big_total[0]);
-        if (st.big_total[1]) atomicAdd(&o.slot->hbig_add, st.big_total[1]);
-        if (st.far_key) atomicMax(&o.slot->min_far_bits, st.far_key);
-        st.mf = st.scanned = 0;
-        st.big_total[0] = st.big_total[1] = 0;
-        st.far_key = 0;
+    if (p.nfar) flush_far(p);
+    const unsigned long long mf = __reduce_add_sync(kFull, (unsigned)p.mf);  // per-lane parts fit 32 bits
+    unsigned long long sc = p.scanned;
+#pragma unroll
+    for (int d = 16; d; d >>= 1) sc += __shfl_xor_sync(kFull, sc, d);
+    const int fk = __reduce_max_sync(kFull, p.far_key);
+    if (lane_id() == 0) {
+        if (mf) atomicAdd(&cc.mf, mf);
+        if (sc) atomicAdd(&cc.scanned, sc);
+        if (p.big_total[0]) atomicAdd(&cc.big_total[0], p.big_total[0]);
+        if (p.big_total[1]) atomicAdd(&cc.big_total[1], p.big_total[1]);
+        if (fk) atomicMax(&cc.far_key, fk);
     }
     __syncthreads();
+    if (threadIdx.x == 0) {
+        Slot *sl = p.o->slot;
+        if (cc.mf) atomicAdd(&sl->mf, cc.mf);
+        if (cc.scanned) atomicAdd(&p.a->ctl->edges_scanned, cc.scanned);
+        if (cc.big_total[0]) atomicAdd(&sl->big_add, cc.big_total[0]);
+        if (cc.big_total[1]) atomicAdd(&sl->hbig_add, cc.big_total[1]);
+        if (cc.far_key) atomicMax(&sl->min_far_bits, cc.far_key);
+        cc.mf = cc.scanned = 0;
+        cc.big_total[0] = cc.big_total[1] = 0;
+        cc.far_key = 0;
+    }
+    // the next phase's pushes are staged only after the grid barrier, which
+    // begins with __syncthreads, so the reset is seen before any reuse
 }
 
-// Expand a frontier (part kPart of each row) in one phase: chunk items (one
-// warp each, kWarps items per CTA iteration), then the short-row queue by CTA
-// tiles (edge-balanced within the tile).  Every lane carries kBatch
-// independent edges per round so their loads and atomics overlap.
+// Expand a frontier (part kPart of each row) in one phase: chunk items one
+// warp each, then the short-row queue in 32-vertex warp tiles (edge-balanced
+// within the tile).  Every lane carries kBatch independent edges per round so
+// their loads and atomics overlap.
 template <int kPart, class Vis>
 __device__ void expand_frontier(const TravArgs &a, const int32_t *q, unsigned nq, const int2 *chunks, unsigned nch,
-                                const Vis &vis, TileShared &ts, Stage &st, const FrontierOut &o)
+                                const Vis &vis, Pusher &p)
 {
     const int lane = (int)lane_id();
-    const unsigned wic = threadIdx.x >> 5;
-    for (unsigned c0 = blockIdx.x * kWarps; c0 < nch; c0 += gridDim.x * kWarps) {
-        const unsigned c = c0 + wic;
-        int u = 0, start = 0, end = 0;
-        float du = 0.0f;
-        if (c < nch) {
-            const int2 it = __ldcg(&chunks[c]);
-            u = it.x;
-            start = it.y;
-            end = min(start + kItem, row_part(a, u, kPart).y);
-            du = vis.begin(u);
-            if (lane == 0) atomicAdd(&st.scanned, (unsigned long long)(end - start));
-        }
-        for (int r = 0; r < kItem; r += 32 * kBatch) {  // same trip count in every warp of the CTA
+    const unsigned gwarp = (blockIdx.x * kBlock + threadIdx.x) >> 5, nwarps = (gridDim.x * kBlock) >> 5;
+    for (unsigned c = gwarp; c < nch; c += nwarps) {
+        const int2 it = chunks[c];
+        const int u = it.x, start = it.y;
+        const int end = min(start + kItem, row_part(a, u, kPart).y);
+        const float du = vis.begin(u);
+        if (lane == 0) p.scanned += (unsigned long long)(end - start);
+        for (int e0 = start; e0 < end; e0 += 32 * kBatch) {
             int us[kBatch], e[kBatch];
             float ds[kBatch];
             bool ok[kBatch];
 #pragma unroll
             for (int j = 0; j < kBatch; j++) {
-                e[j] = start + r + lane + 32 * j;
+                e[j] = e0 + lane + 32 * j;
                 ok[j] = e[j] < end;
                 us[j] = u;
                 ds[j] = du;
             }
-            if (__any_sync(kFull, ok[0])) vis.visit_batch(us, ds, e, ok, st);
-            stage_flush(a, st, ts, o, false);
+            vis.visit_batch(us, ds, e, ok, p);
         }
     }
-    for (unsigned tile = blockIdx.x * kBlock; tile < nq; tile += gridDim.x * kBlock) {
-        const unsigned i = tile + threadIdx.x;
+    WarpStage *s = p.s;
+    for (unsigned t0 = gwarp * 32; t0 < nq; t0 += nwarps * 32) {
+        const unsigned i = t0 + lane;
         int u = 0, rb = 0, deg = 0;
         if (i < nq) {
-            u = __ldcg(&q[i]);
-            const int2 p = row_part(a, u, kPart);
-            rb = p.x;
-            deg = p.y - p.x;
+            u = q[i];
+            const int2 pr = row_part(a, u, kPart);
+            rb = pr.x;
+            deg = pr.y - pr.x;
         }
-        const int pre = block_excl_scan(deg, ts);
-        ts.u[threadIdx.x] = u;
-        ts.rb[threadIdx.x] = rb;
-        ts.pre[threadIdx.x] = pre;
-        ts.du[threadIdx.x] = deg > 0 ? vis.begin(u) : 0.0f;
-        __syncthreads();
-        const int total = ts.total;
-        if (threadIdx.x == 0 && total) atomicAdd(&st.scanned, (unsigned long long)total);
-        const int n = (int)min((unsigned)kBlock, nq - tile);
-        for (int base = 0; base < total; base += kRoundPush) {
+        int incl = deg;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int y = __shfl_up_sync(kFull, incl, d);
+            if (lane >= d) incl += y;
+        }
+        const int total = __shfl_sync(kFull, incl, 31);
+        s->tu[lane] = u;
+        s->trb[lane] = rb;
+        s->tpre[lane] = incl - deg;
+        s->tdu[lane] = deg > 0 ? vis.begin(u) : 0.0f;
+        __syncwarp();
+        if (lane == 0) p.scanned += (unsigned long long)total;
+        const int n = (int)min(32u, nq - t0);
+        for (int base = 0; base < total; base += 32 * kBatch) {
             int us[kBatch], e[kBatch];
             float ds[kBatch];
             bool ok[kBatch];
 #pragma unroll
             for (int j = 0; j < kBatch; j++) {
-                const int k = base + (int)threadIdx.x + kBlock * j;
+                const int k = base + lane + 32 * j;
                 ok[j] = k < total;
                 int lo = 0;
                 if (ok[j]) {
                     int hi = n;
                     while (hi - lo > 1) {
                         const int mid = (lo + hi) >> 1;
-                        if (ts.pre[mid] <= k) lo = mid;
+                        if (s->tpre[mid] <= k) lo = mid;
                         else hi = mid;
                     }
                 }
-                e[j] = ts.rb[lo] + (k - ts.pre[lo]);
-                us[j] = ts.u[lo];
-                ds[j] = ts.du[lo];
+                e[j] = s->trb[lo] + (k - s->tpre[lo]);
+                us[j] = s->tu[lo];
+                ds[j] = s->tdu[lo];
             }
-            // lanes whose first edge is past the end have none at all
-            if (__any_sync(kFull, ok[0])) vis.visit_batch(us, ds, e, ok, st);
-            stage_flush(a, st, ts, o, false);
+            vis.visit_batch(us, ds, e, ok, p);
         }
-        __syncthreads();
+        __syncwarp();
     }
-    stage_flush(a, st, ts, o, true);
 }
 
 // One vertex as a frontier of its own (row part [rb, re)): every CTA computes
@@ -638,7 +664,7 @@ struct BfsPush {
     __device__ __forceinline__ float begin(int) const { return 0.0f; }
 
     __device__ __forceinline__ void visit_batch(const int (&)[kBatch], const float (&)[kBatch], const int (&e)[kBatch],
-                                                const bool (&ok)[kBatch], Stage &st) const
+                                                const bool (&ok)[kBatch], Pusher &p) const
     {
         int v[kBatch];
         unsigned word[kBatch];
@@ -653,7 +679,7 @@ struct BfsPush {
             fresh[j] = false;
             if (!(word[j] & bit)) fresh[j] = !(atomicOr(a->visited + (v[j] >> 5), bit) & bit);
         }
-        unsigned deg[kBatch], dsum = 0;
+        unsigned deg[kBatch];
 #pragma unroll
         for (int j = 0; j < kBatch; j++) {
             deg[j] = 0;
@@ -661,11 +687,10 @@ struct BfsPush {
                 reinterpret_cast<int *>(a->value)[v[j]] = level_next;
                 deg[j] = (unsigned)(__ldg(&a->out_off[v[j] + 1]) - __ldg(&a->out_off[v[j]]));
             }
-            dsum += deg[j];
+            p.mf += deg[j];
         }
 #pragma unroll
-        for (int j = 0; j < kBatch; j++) stage_push(st, 0, fresh[j], v[j], deg[j]);
-        stage_add_mf(st, dsum);
+        for (int j = 0; j < kBatch; j++) push(p, 0, fresh[j], v[j], deg[j]);
     }
 };
 
@@ -683,7 +708,7 @@ struct SsspPush {
     __device__ __forceinline__ float begin(int u) const { return __uint_as_float(__ldcg(&a->value[u])); }
 
     __device__ __forceinline__ void visit_batch(const int (&)[kBatch], const float (&du)[kBatch],
-                                                const int (&e)[kBatch], const bool (&ok)[kBatch], Stage &st) const
+                                                const int (&e)[kBatch], const bool (&ok)[kBatch], Pusher &p) const
     {
         int v[kBatch];
         float nd[kBatch];
@@ -733,26 +758,37 @@ struct SsspPush {
         }
 #pragma unroll
         for (int j = 0; j < kBatch; j++) {
-            stage_push(st, 0, light[j], v[j], (unsigned)nl[j]);
-            stage_push(st, 1, heavy[j], v[j], (unsigned)nh[j]);
-            stage_far(st, far[j], v[j], far[j] ? 0x7fffffff - __float_as_int(nd[j]) : 0);
+            push(p, 0, light[j], v[j], (unsigned)nl[j]);
+            push(p, 1, heavy[j], v[j], (unsigned)nh[j]);
+            push_far(p, far[j], v[j], far[j] ? 0x7fffffff - __float_as_int(nd[j]) : 0);
         }
     }
 };
 
-// --------------------------------------------------------------- BFS kernel
-__global__ void __launch_bounds__(kBlock) bfs_persistent(TravArgs a)
+__device__ __forceinline__ void init_counters(CtaCounters &cc)
 {
-    __shared__ TileShared ts;
-    __shared__ Stage st;
+    if (threadIdx.x == 0) {
+        cc.mf = cc.scanned = 0;
+        cc.big_total[0] = cc.big_total[1] = 0;
+        cc.far_key = 0;
+    }
+    __syncthreads();
+}
+
+// --------------------------------------------------------------- BFS kernel
+__global__ void __launch_bounds__(kBlock, 5) bfs_persistent(TravArgs a)
+{
+    __shared__ WarpStage wst[kWarps];
+    __shared__ CtaCounters cc;
     __shared__ int s_dir;
     Ctl *ctl = a.ctl;
     const int gtid = blockIdx.x * kBlock + threadIdx.x, nth = gridDim.x * kBlock;
-    const unsigned gwarp = gtid >> 5, nwarps = nth >> 5, wic = threadIdx.x >> 5;
+    const unsigned gwarp = gtid >> 5, nwarps = nth >> 5;
+    WarpStage *mys = &wst[threadIdx.x >> 5];
     const int s = a.source;
     int ph = 0;
 
-    stage_init(st);
+    init_counters(cc);
     for (int v = gtid; v < a.V; v += nth) reinterpret_cast<int *>(a.value)[v] = v == s ? 0 : -1;
     for (int w = gtid; w < a.W; w += nth) a.visited[w] = w == (s >> 5) ? 1u << (s & 31) : 0u;
     unsigned nq, nch;
@@ -793,7 +829,7 @@ __global__ void __launch_bounds__(kBlock) bfs_persistent(TravArgs a)
             clear_ahead(ctl, ph);
             for (unsigned w = gwarp; w < (unsigned)a.W; w += nwarps) {
                 const int v = (int)(w * 32 + lane_id());
-                const bool f = v < a.V && (int)__ldcg(&a.value[v]) == L;
+                const bool f = v < a.V && (int)a.value[v] == L;
                 const unsigned m = __ballot_sync(kFull, f);
                 if (lane_id() == 0) (fcur ? a.front1 : a.front0)[w] = m;
             }
@@ -804,78 +840,75 @@ __global__ void __launch_bounds__(kBlock) bfs_persistent(TravArgs a)
         clear_ahead(ctl, ph);
         const FrontierOut out{{(cur ? a.q0 : a.q1), nullptr}, {(cur ? a.chunks0 : a.chunks1), nullptr}, {0u, 0u},
                               {0u, 0u}, {kPartWhole, kPartWhole}, nullptr, 0u, &ctl->slot[ph % kSlots]};
+        Pusher p = make_pusher(a, out, mys);
         if (dir == 0) {
             const BfsPush vis{&a, L + 1};
-            expand_frontier<kPartWhole>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, ts, st, out);
+            expand_frontier<kPartWhole>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, p);
         } else {
-            // bottom-up: each warp owns 32 vertices = one bitmap word; kWarps words per CTA iteration
+            // bottom-up: each warp owns 32 vertices = one bitmap word
             const unsigned *fc = fcur ? a.front1 : a.front0;
             unsigned *fn = fcur ? a.front0 : a.front1;
-            for (unsigned w0 = blockIdx.x * kWarps; w0 < (unsigned)a.W; w0 += gridDim.x * kWarps) {
-                const unsigned w = w0 + wic;
-                if (w < (unsigned)a.W) {
-                    // The frontier bitmap and this word of `visited` were written in
-                    // earlier phases and only this warp writes the word now: plain
-                    // (L1-cacheable) loads are coherent after the grid barrier.
-                    const int lane = (int)lane_id();
-                    const int v = (int)(w * 32 + lane);
-                    const unsigned vis = a.visited[w];
-                    bool cand = v < a.V && !((vis >> lane) & 1u);
-                    int k = 0, kend = 0;
-                    if (cand) {
-                        k = __ldg(&a.in_off[v]);
-                        kend = __ldg(&a.in_off[v + 1]);
-                    }
-                    bool found = false;
-                    // long in-rows: the whole warp scans one row 32 entries at a time
-                    unsigned coop = __ballot_sync(kFull, cand && kend - k > 32);
-                    while (coop) {
-                        const int owner = __ffs(coop) - 1;
-                        coop &= coop - 1;
-                        const int kb = __shfl_sync(kFull, k, owner), ke = __shfl_sync(kFull, kend, owner);
-                        bool hit = false;
-                        for (int kk = kb + lane; kk - lane < ke; kk += 32) {
-                            bool h = false;
-                            if (kk < ke) {
-                                const int u = __ldg(&a.in_adj[kk]);
-                                h = (fc[u >> 5] >> (u & 31)) & 1u;
-                            }
-                            if (__any_sync(kFull, h)) {
-                                hit = true;
-                                break;
-                            }
-                        }
-                        if (lane == owner) {
-                            found = hit;
-                            cand = false;
-                        }
-                    }
-                    // short in-rows: one lane each
-                    if (cand) {
-                        for (; k < kend; k++) {
-                            const int u = __ldg(&a.in_adj[k]);
-                            if ((fc[u >> 5] >> (u & 31)) & 1u) { found = true; break; }
-                        }
-                    }
-                    const unsigned m = __ballot_sync(kFull, found);
-                    if (lane_id() == 0) {
-                        fn[w] = m;
-                        if (m) a.visited[w] = vis | m;
-                    }
-                    unsigned deg = 0;
-                    if (found) {
-                        reinterpret_cast<int *>(a.value)[v] = L + 1;
-                        deg = (unsigned)(__ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v]));
-                    }
-                    stage_push(st, 0, found, v, deg);
-                    stage_add_mf(st, deg);
+            for (unsigned w = gwarp; w < (unsigned)a.W; w += nwarps) {
+                // The frontier bitmap and this word of `visited` were written in
+                // earlier phases and only this warp writes the word now: plain
+                // (L1-cacheable) loads are coherent after the grid barrier.
+                const int lane = (int)lane_id();
+                const int v = (int)(w * 32 + lane);
+                const unsigned vis = a.visited[w];
+                bool cand = v < a.V && !((vis >> lane) & 1u);
+                int k = 0, kend = 0;
+                if (cand) {
+                    k = __ldg(&a.in_off[v]);
+                    kend = __ldg(&a.in_off[v + 1]);
                 }
-                stage_flush(a, st, ts, out, false);
+                bool found = false;
+                // long in-rows: the whole warp scans one row 32 entries at a time
+                unsigned coop = __ballot_sync(kFull, cand && kend - k > 32);
+                while (coop) {
+                    const int owner = __ffs(coop) - 1;
+                    coop &= coop - 1;
+                    const int kb = __shfl_sync(kFull, k, owner), ke = __shfl_sync(kFull, kend, owner);
+                    bool hit = false;
+                    for (int kk = kb + lane; kk - lane < ke; kk += 32) {
+                        bool h = false;
+                        if (kk < ke) {
+                            const int u = __ldg(&a.in_adj[kk]);
+                            h = (fc[u >> 5] >> (u & 31)) & 1u;
+                        }
+                        if (__any_sync(kFull, h)) {
+                            hit = true;
+                            break;
+                        }
+                    }
+                    if (lane == owner) {
+                        found = hit;
+                        cand = false;
+                    }
+                }
+                // short in-rows: one lane each
+                if (cand) {
+                    for (; k < kend; k++) {
+                        const int u = __ldg(&a.in_adj[k]);
+                        if ((fc[u >> 5] >> (u & 31)) & 1u) { found = true; break; }
+                    }
+                }
+                const unsigned m = __ballot_sync(kFull, found);
+                if (lane == 0) {
+                    fn[w] = m;
+                    if (m) a.visited[w] = vis | m;
+                }
+                unsigned deg = 0;
+                if (found) {
+                    reinterpret_cast<int *>(a.value)[v] = L + 1;
+                    deg = (unsigned)(__ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v]));
+                }
+                p.mf += deg;
+                push(p, 0, found, v, deg);
             }
-            stage_flush(a, st, ts, out, true);
             fcur ^= 1;
             bu_steps++;
         }
+        finish_phase(p, cc);
         if (!grid_sync(ctl, a.timeout_ns, ph)) return;
         log_phase(ctl, dir, (unsigned)nf);
         const SlotView s0 = read_slot(ctl, ph);
@@ -913,16 +946,18 @@ __global__ void __launch_bounds__(kBlock) bfs_persistent(TravArgs a)
 // delta = +inf is Bellman-Ford over active vertices (every edge light).  Any
 // order of relaxations reaches the same fixpoint bits: fl(x + w) is monotone
 // in x and not below x for w >= 0.
-__global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
+__global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
 {
-    __shared__ TileShared ts;
-    __shared__ Stage st;
+    __shared__ WarpStage wst[kWarps];
+    __shared__ CtaCounters cc;
     __shared__ float s_delta;
     Ctl *ctl = a.ctl;
     const int gtid = blockIdx.x * kBlock + threadIdx.x, nth = gridDim.x * kBlock;
+    const unsigned gwarp = gtid >> 5, nwarps = nth >> 5;
+    WarpStage *mys = &wst[threadIdx.x >> 5];
     const int lpart = a.nlight ? kPartLight : kPartWhole;
     int ph = 0;
-    stage_init(st);
+    init_counters(cc);
     // Stamp ids continue across queries so the stamp arrays need no clearing;
     // every CTA reads the base before the first barrier, thread 0 of CTA 0
     // advances it after the last one.  Near the int range they are recycled.
@@ -968,15 +1003,15 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
         clear_ahead(ctl, ph);
         const FrontierOut out{{a.q0, nullptr}, {a.chunks0, nullptr}, {0u, 0u}, {0u, 0u}, {kPartWhole, kPartWhole},
                               nullptr, 0u, &ctl->slot[ph % kSlots]};
-        for (int base = blockIdx.x * kBlock; base < a.V; base += gridDim.x * kBlock) {
-            const int v = base + (int)threadIdx.x;
+        Pusher p = make_pusher(a, out, mys);
+        for (unsigned base = gwarp * 32; base < (unsigned)a.V; base += nwarps * 32) {
+            const int v = (int)(base + lane_id());
             const bool act = v < a.V && __ldcg(&a.value[v]) < kFltMaxBits;
             if (act) a.stamp_near[v] = near_id;
             const unsigned deg = act ? (unsigned)(__ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v])) : 0u;
-            stage_push(st, 0, act && deg > 0, v, deg);
-            stage_flush(a, st, ts, out, false);
+            push(p, 0, act && deg > 0, v, deg);
         }
-        stage_flush(a, st, ts, out, true);
+        finish_phase(p, cc);
         if (!grid_sync(ctl, a.timeout_ns, ph)) return;
         const SlotView s0 = read_slot(ctl, ph);
         nq = s0.q_add;
@@ -1003,11 +1038,13 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
                                   (fcur ? a.far1 : a.far0),
                                   (unsigned)far_len,
                                   &ctl->slot[ph % kSlots]};
+            Pusher p = make_pusher(a, out, mys);
             const SsspPush vis{&a, thr, near_id + 1, heavy_id, far_id};
             if (lpart == kPartLight)
-                expand_frontier<kPartLight>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, ts, st, out);
+                expand_frontier<kPartLight>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, p);
             else
-                expand_frontier<kPartWhole>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, ts, st, out);
+                expand_frontier<kPartWhole>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, p);
+            finish_phase(p, cc);
             if (!grid_sync(ctl, a.timeout_ns, ph)) return;
             log_phase(ctl, 3, nq + nbig);
             const SlotView s0 = read_slot(ctl, ph);
@@ -1035,8 +1072,10 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
                                   (fcur ? a.far1 : a.far0),
                                   (unsigned)far_len,
                                   &ctl->slot[ph % kSlots]};
+            Pusher p = make_pusher(a, out, mys);
             const SsspPush vis{&a, thr, near_id, heavy_id + 1, far_id};
-            expand_frontier<kPartHeavy>(a, (hcur ? a.hq1 : a.hq0), hq, (hcur ? a.hch1 : a.hch0), hch, vis, ts, st, out);
+            expand_frontier<kPartHeavy>(a, (hcur ? a.hq1 : a.hq0), hq, (hcur ? a.hch1 : a.hch0), hch, vis, p);
+            finish_phase(p, cc);
             if (!grid_sync(ctl, a.timeout_ns, ph)) return;
             log_phase(ctl, 5, hq + hbig);
             const SlotView s0 = read_slot(ctl, ph);
@@ -1081,11 +1120,12 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
                                   (fcur ? a.far0 : a.far1),
                                   0u,
                                   &ctl->slot[ph % kSlots]};
-            for (unsigned long long base = (unsigned long long)blockIdx.x * kBlock; base < far_len;
-                 base += (unsigned long long)gridDim.x * kBlock) {
-                const unsigned long long i = base + threadIdx.x;
+            Pusher p = make_pusher(a, out, mys);
+            for (unsigned long long base = (unsigned long long)gwarp * 32; base < far_len;
+                 base += (unsigned long long)nwarps * 32) {
+                const unsigned long long i = base + lane_id();
                 const bool valid = i < far_len;
-                const int v = valid ? __ldcg(&fp[i]) : 0;
+                const int v = valid ? fp[i] : 0;
                 const float d = valid ? __uint_as_float(__ldcg(&a.value[v])) : 0.0f;
                 const bool in_bucket = valid && d >= told && d < thr;
                 int nl = 0, nh = 0;
@@ -1097,12 +1137,11 @@ __global__ void __launch_bounds__(kBlock) sssp_persistent(TravArgs a)
                 const bool light = in_bucket && nl > 0 && atomicExch(&a.stamp_near[v], near_id) != near_id;
                 const bool heavy = in_bucket && nh > 0 && atomicExch(&a.stamp_heavy[v], heavy_id) != heavy_id;
                 const bool keep = valid && d >= thr && atomicExch(&a.stamp_far[v], far_id) != far_id;
-                stage_push(st, 0, light, v, (unsigned)nl);
-                stage_push(st, 1, heavy, v, (unsigned)nh);
-                stage_far(st, keep, v, keep ? 0x7fffffff - __float_as_int(d) : 0);
-                stage_flush(a, st, ts, out, false);
+                push(p, 0, light, v, (unsigned)nl);
+                push(p, 1, heavy, v, (unsigned)nh);
+                push_far(p, keep, v, keep ? 0x7fffffff - __float_as_int(d) : 0);
             }
-            stage_flush(a, st, ts, out, true);
+            finish_phase(p, cc);
             if (!grid_sync(ctl, a.timeout_ns, ph)) return;
             log_phase(ctl, 4, (unsigned)far_len);
             const SlotView s0 = read_slot(ctl, ph);
