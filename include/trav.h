@@ -235,6 +235,15 @@ int trav_mlp_loss_grad(int32_t kind, const float *params, const float *x, const 
 int trav_mlp_train(int32_t kind, float *params, const float *x, const int32_t *labels, int32_t n, int32_t epochs,
                    float lr, float *final_loss);
 
+/* Launch shape of the following queries of one kind on this handle: the
+ * persistent kernel runs `ctas` CTAs of 256 threads (1 <= ctas <= the number
+ * the device can hold at once, which *max_ctas receives when not NULL);
+ * ctas == 0 restores that maximum.  Results do not depend on it; small graphs
+ * and long chains of small steps can run faster on fewer CTAs, because every
+ * step ends with a grid barrier that all CTAs join.  No counterpart in the
+ * reference. */
+int trav_set_grid(trav_graph *g, int32_t kind, int32_t ctas, int32_t *max_ctas);
+
 /* Force the schedule's decisions for the following queries of one kind on
  * this handle (used to time alternatives when building training traces):
  * decision i takes option plan[i] when plan[i] < 255 and follows the schedule

@@ -404,6 +404,20 @@ int trav_graph_set_stream(trav_graph *g, void *stream)
     return TRAV_OK;
 }
 
+int trav_set_grid(trav_graph *g, int32_t kind, int32_t ctas, int32_t *max_ctas)
+{
+    if (!g) return bad("graph handle is NULL");
+    if (kind != 0 && kind != 1) return bad("kind must be 0 (BFS) or 1 (SSSP)");
+    TRY_CUDA(cudaSetDevice(g->device));
+    const int most = persistent_grid_size(kind);
+    if (most <= 0) return TRAV_ERR_CUDA;
+    if (max_ctas) *max_ctas = most;
+    if (ctas < 0 || ctas > most) return bad("ctas must lie in [0, the co-resident maximum]");
+    TRY_CUDA(cudaStreamSynchronize(g->st));
+    g->ws.grid[kind] = ctas;
+    return TRAV_OK;
+}
+
 int trav_set_plan(trav_graph *g, int32_t kind, const uint8_t *plan, int32_t n)
 {
     if (!g) return bad("graph handle is NULL");
@@ -546,7 +560,7 @@ int trav_bellman_ford_el_f32(const int32_t *src, const int32_t *dst, const float
     TRY(build_graph_device(vertices, edges, src, dst, w, h->st, &h->g));
     TRY(workspace_ensure(&h->ws, h->g, 1, h->st));
     gather_bits_kernel<<<(vertices + 255) / 256 < 4096 ? (vertices + 255) / 256 : 4096, 256, 0, h->st>>>(
-        h->ws.value, d, h->g.old_of_new, vertices);
+        reinterpret_cast<unsigned *>(h->ws.queue[1]), d, h->g.old_of_new, vertices);
     TRY_CUDA(cudaGetLastError());
     TRY(launch_sssp(h->g, &h->ws, 0, -1, INFINITY, nullptr, d, 1, h->st, nullptr, nullptr));
     TRY_CUDA(cudaStreamSynchronize(h->st));

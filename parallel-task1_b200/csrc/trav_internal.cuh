@@ -19,6 +19,14 @@ constexpr int kMaxTrace = 4096;   // steps recorded per query
 constexpr int kMaxDec = 1024;     // schedule decisions recorded per query
 constexpr int kDecFeat = 10;      // features per decision (the schedule MLP's input width)
 constexpr int kSlots = 4;         // ring of per-phase counter slots
+// Row-class flags in the low word of an SSSP packed distance: which parts of
+// the vertex's out-row are non-empty and which are longer than kSmallDeg.  They
+// depend only on the graph and delta, so a 64-bit atomicMin keeps them.
+constexpr unsigned kClsLight = 1, kClsLightBig = 2, kClsHeavy = 4, kClsHeavyBig = 8;
+
+// Words per SSSP dedupe bitmap: W rounded up to 16 bytes, so each bitmap can
+// be cleared with 16-byte stores.
+__host__ __device__ inline int32_t bitmap_stride(int32_t W) { return (W + 3) & ~3; }
 
 // Device status codes written to Ctl::err.
 constexpr int kErrTimeout = 1;    // a bounded grid-barrier wait gave up
@@ -35,35 +43,29 @@ struct Slot {
     unsigned int hq_add;          // SSSP heavy list: short heavy parts appended
     unsigned int hchunk_add;      // SSSP heavy list: chunk items appended
     unsigned int hbig_add;        // SSSP heavy list: vertices pushed as chunk items
+    unsigned long long scanned;   // out-edges expanded in the phase
 };
-
-constexpr int kBarGroups = 32;    // first level of the grid barrier
-
-// One barrier arrival counter per 128-byte line (no two groups share a line).
-struct alignas(128) BarGroup {
-    unsigned int count;
-};
+static_assert(sizeof(Slot) == 48 && offsetof(Slot, mf) == 16 && offsetof(Slot, scanned) == 40,
+              "grid_sync reads Slot as twelve 32-bit words");
 
 // Control block of one persistent launch (zeroed by the host before launch).
 struct Ctl {
-    unsigned int bar_count;
-    unsigned int bar_gen;
+    unsigned long long bar_count;  // grid-barrier arrivals so far (only grows during a launch)
     int err;
     int err_phase;
-    BarGroup bar_group[kBarGroups];
     Slot slot[kSlots];
     // written by CTA 0 as the query runs
     int steps;
     int buckets;
     int bottom_up_steps;
-    int next_id;                  // first unused stamp id after the query
     unsigned long long edges_scanned;  // out-edges expanded (push-side work, all steps)
     int nphase;                   // phases logged below
     int ndec;                     // schedule decisions logged below
     unsigned char dirs[kMaxTrace];       // BFS: direction of step s (0 top-down, 1 bottom-up)
     unsigned int frontier[kMaxTrace];    // BFS: frontier size of step s; SSSP: of expansion s
     // phase log (CTA 0, after each grid barrier): kind (0 top-down, 1 bottom-up,
-    // 2 bitmap build, 3 relaxation round, 4 bucket opening), frontier size,
+    // 2 bitmap build, 3 light relaxation round, 4 bucket opening, 5 heavy
+    // relaxation round), frontier size,
     // %globaltimer at the phase's end and cumulative edges_scanned
     unsigned char ph_kind[kMaxTrace];
     unsigned int ph_size[kMaxTrace];
@@ -96,14 +98,14 @@ struct DevGraph {
 struct Workspace {
     int32_t V = 0;
     int64_t chunk_cap = 0;
-    unsigned int *value = nullptr;     // V: BFS level (int32) or SSSP distance bits
+    // V 64-bit words: BFS levels (int32, the first V words) or SSSP packed
+    // distances (float bits << 32 | row-class flags, see kCls*)
+    unsigned int *value = nullptr;
     unsigned int *visited = nullptr;   // W words
     unsigned int *front[2] = {nullptr, nullptr};  // W words each
     int32_t *queue[2] = {nullptr, nullptr};       // V each
     int32_t *far[2] = {nullptr, nullptr};         // V each
-    int32_t *stamp_near = nullptr;     // V
-    int32_t *stamp_far = nullptr;      // V
-    int32_t *stamp_heavy = nullptr;    // V
+    unsigned int *bmap = nullptr;      // 6 W-word dedupe bitmaps (SSSP): near[2], heavy[2], far[2]
     int32_t *hq[2] = {nullptr, nullptr};  // SSSP heavy lists (short heavy parts), V each
     int2 *hchunks[2] = {nullptr, nullptr};  // SSSP heavy lists (chunk items), chunk_cap each
     int32_t *nlight = nullptr;         // V: out-edges lighter than nlight_delta (rows are sorted by weight)
@@ -111,9 +113,9 @@ struct Workspace {
     int2 *chunks[2] = {nullptr, nullptr};  // chunk_cap items each (current / next frontier)
     Ctl *ctl = nullptr;                // ctl_cap control blocks: one per query of a batch
     int ctl_cap = 0;
-    int *id_base = nullptr;            // device: first unused stamp id (continues across queries)
     unsigned char *plan[2] = {nullptr, nullptr};  // forced decisions for BFS / SSSP queries (device)
     int plan_len[2] = {0, 0};
+    int grid[2] = {0, 0};              // CTAs of the BFS / SSSP launches (0 = as many as fit)
 };
 
 // Arguments of the persistent kernels (passed by value).
@@ -129,12 +131,13 @@ struct TravArgs {
     int32_t W;        // bitmap words
     int64_t E;
     // workspace
-    unsigned int *value;
+    unsigned int *value;        // BFS levels
+    unsigned long long *dist;   // SSSP packed distances (same memory as value)
     unsigned int *visited;
     unsigned int *front0, *front1;
     int32_t *q0, *q1;
     int32_t *far0, *far1;
-    int32_t *stamp_near, *stamp_far, *stamp_heavy;
+    unsigned int *bmap;       // SSSP dedupe bitmaps: near[2], heavy[2], far[2], W words each
     int32_t *hq0, *hq1;       // SSSP heavy lists
     int2 *hch0, *hch1;
     const int32_t *__restrict__ nlight;  // light-prefix length per vertex; nullptr = every edge is light
@@ -142,9 +145,9 @@ struct TravArgs {
     int2 *chunks0, *chunks1;  // chunk items of the current / next frontier (one-phase expansion)
     Ctl *ctl;
     // query
-    int32_t source;        // new id; -1 = start from the distances in `value`
+    int32_t source;        // new id; -1 = start from the distance bits in init_bits
+    const unsigned int *init_bits;  // source -1: V distance bits (new ids), read before the first barrier
     int32_t max_steps;
-    int *id_base;          // device: first stamp id this query may use; updated at the end
     // BFS options
     float alpha, beta;
     int32_t force_dir;

@@ -36,13 +36,6 @@ __device__ __forceinline__ unsigned long long globaltimer()
     return t;
 }
 
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
-{
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
 __device__ __forceinline__ int ld_relaxed_int(const int *p)
 {
     int v;
@@ -53,55 +46,11 @@ __device__ __forceinline__ int ld_relaxed_int(const int *p)
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
 
-// Grid-wide barrier with a bounded wait.  Thread 0 of CTA b arrives on group
-// counter b % kBarGroups (one 128-byte line each, so arrivals of different
-// groups do not serialise on one address); the last arriver of a group resets
-// it and arrives on the top counter; the last top arriver resets that and
-// advances the generation, which every waiter polls.  Waiters give up after
-// timeout_ns (or when another CTA already failed) and the barrier then
-// returns false in every thread of the CTA.
-__device__ bool grid_sync(Ctl *ctl, unsigned long long timeout_ns, int phase)
+__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned *p)
 {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        const unsigned nb = gridDim.x;
-        const unsigned groups = nb < (unsigned)kBarGroups ? nb : (unsigned)kBarGroups;
-        const unsigned g = blockIdx.x % groups;
-        const unsigned in_group = (nb - g + groups - 1) / groups;  // CTAs b < nb with b % groups == g
-        unsigned gen = ld_acquire(&ctl->bar_gen);
-        __threadfence();
-        bool last = false;
-        if (atomicAdd(&ctl->bar_group[g].count, 1u) == in_group - 1) {
-            atomicExch(&ctl->bar_group[g].count, 0u);
-            __threadfence();  // order the group's arrivals before the top arrival
-            last = atomicAdd(&ctl->bar_count, 1u) == groups - 1;
-        }
-        if (last) {
-            atomicExch(&ctl->bar_count, 0u);
-            __threadfence();
-            atomicAdd(&ctl->bar_gen, 1u);
-        } else {
-            unsigned long long t0 = globaltimer();
-            unsigned ns = 32;
-            while (ld_acquire(&ctl->bar_gen) == gen) {
-                if (ld_relaxed_int(&ctl->err) != 0) { ok = 0; break; }
-                __nanosleep(ns);
-                if (ns < 256) ns <<= 1;
-                if (globaltimer() - t0 > timeout_ns) {
-                    if (atomicCAS(&ctl->err, 0, kErrTimeout) == 0) atomicExch(&ctl->err_phase, phase);
-                    ok = 0;
-                    break;
-                }
-            }
-        }
-        __threadfence();
-        if (ld_relaxed_int(&ctl->err) != 0) ok = 0;
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
 }
 
 struct SlotView {
@@ -110,7 +59,80 @@ struct SlotView {
     unsigned long long mf;
     unsigned big_add;
     unsigned hq_add, hchunk_add, hbig_add;
+    unsigned long long scanned;
 };
+
+// Grid-wide barrier with a bounded wait.  After the CTA barrier, thread 0 of
+// every CTA adds one to a single arrival counter with an acquire-release
+// atomic (which orders the CTA's writes of the phase before it).  The counter
+// only grows, so barrier k of a launch is passed once it reaches
+// k * gridDim.x: there is no reset and no generation word, and the critical
+// path is one arrival plus one poll.  (A tree of reset counters puts a chain of
+// dependent atomics and fences on that path instead.)  Waiters poll with an
+// acquire load and give up after timeout_ns, or when another CTA already
+// failed; the barrier then returns false in every thread of the CTA.
+//
+// With `view`, warp 0 also reads the counter slot of `phase` once for the
+// whole CTA (one coalesced load) and leaves it decoded in shared memory: if
+// every warp read the slot itself, the thousands of requests to one L2 line
+// after each barrier would cost as much as a small phase.
+__device__ bool grid_sync(Ctl *ctl, unsigned long long timeout_ns, int phase, SlotView *view = nullptr)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        if (threadIdx.x == 0) {
+            int ok = 1;
+            const unsigned long long nb = gridDim.x;
+            unsigned long long old;
+            asm volatile("atom.add.acq_rel.gpu.global.u64 %0, [%1], 1;" : "=l"(old) : "l"(&ctl->bar_count) : "memory");
+            const unsigned long long target = (old / nb + 1) * nb;
+            if (old + 1 != target) {
+                const unsigned long long t0 = globaltimer();
+                unsigned ns = 32;
+                while (true) {
+                    unsigned long long c;
+                    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(c) : "l"(&ctl->bar_count) : "memory");
+                    if (c >= target) break;
+                    if (ld_relaxed_int(&ctl->err) != 0) { ok = 0; break; }
+                    __nanosleep(ns);
+                    if (ns < 128) ns <<= 1;
+                    if (globaltimer() - t0 > timeout_ns) {
+                        if (atomicCAS(&ctl->err, 0, kErrTimeout) == 0) atomicExch(&ctl->err_phase, phase);
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+            s_ok = ok;
+        }
+        __syncwarp();
+        if (view) {
+            // Slot is 48 bytes: lanes 0-11 load one word each
+            const unsigned lane = threadIdx.x;
+            const unsigned *w = reinterpret_cast<const unsigned *>(&ctl->slot[phase % kSlots]);
+            const unsigned x = lane < sizeof(Slot) / 4 ? ld_relaxed_u32(w + lane) : 0u;
+            unsigned f[12];
+#pragma unroll
+            for (int k = 0; k < 12; k++) f[k] = __shfl_sync(kFull, x, k);
+            if (lane == 0) {
+                view->q_add = f[0];
+                view->far_add = f[1];
+                view->chunk_add = f[2];
+                const int neg = (int)f[3];  // stored as 0x7fffffff - bits via atomicMax
+                view->min_far_bits = neg > 0 ? 0x7fffffff - neg : (int)kFltMaxBits;
+                view->mf = (unsigned long long)f[4] | ((unsigned long long)f[5] << 32);
+                view->big_add = f[6];
+                view->hq_add = f[7];
+                view->hchunk_add = f[8];
+                view->hbig_add = f[9];
+                view->scanned = (unsigned long long)f[10] | ((unsigned long long)f[11] << 32);
+            }
+        }
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
 
 __device__ __forceinline__ SlotView read_slot(const Ctl *ctl, int ph)
 {
@@ -126,6 +148,7 @@ __device__ __forceinline__ SlotView read_slot(const Ctl *ctl, int ph)
     v.hq_add = s->hq_add;
     v.hchunk_add = s->hchunk_add;
     v.hbig_add = s->hbig_add;
+    v.scanned = s->scanned;
     return v;
 }
 
@@ -144,6 +167,7 @@ __device__ __forceinline__ void clear_ahead(Ctl *ctl, int ph)
         s->hq_add = 0;
         s->hchunk_add = 0;
         s->hbig_add = 0;
+        s->scanned = 0;
     }
 }
 
@@ -154,35 +178,47 @@ __device__ __forceinline__ int planned(const TravArgs &a, int i)
     return (a.plan && i < a.plan_len && a.plan[i] != 255) ? (int)a.plan[i] : -1;
 }
 
-__device__ __forceinline__ void log_decision(Ctl *ctl, const Feat &f, int choice, float lo, float hi)
+// Log counters.  Every thread that calls the log functions keeps them in
+// registers; thread 0 of CTA 0 writes the logs with plain stores, so logging
+// adds no load to the step's critical path (every CTA waits for CTA 0 at the
+// next barrier).
+struct PhaseLog {
+    int nphase = 0, ndec = 0;
+    unsigned long long scanned = 0;  // edges expanded so far (sum of the slots' counts)
+};
+
+__device__ __forceinline__ void log_decision(Ctl *ctl, PhaseLog &lg, const Feat &f, int choice, float lo, float hi)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        const int i = ctl->ndec;
+        const int i = lg.ndec;
         if (i < kMaxDec) {
 #pragma unroll
             for (int k = 0; k < kDecFeat; k++) ctl->dec_x[i][k] = f.x[k];
             ctl->dec_choice[i] = (unsigned char)choice;
-            ctl->dec_phase[i] = ctl->nphase;
+            ctl->dec_phase[i] = lg.nphase;
             ctl->dec_lo[i] = lo;
             ctl->dec_hi[i] = hi;
         }
         ctl->ndec = i + 1;
     }
+    lg.ndec++;
 }
 
 // Phase log entry, written by CTA 0 thread 0 right after a grid barrier.
-__device__ __forceinline__ void log_phase(Ctl *ctl, int kind, unsigned size)
+__device__ __forceinline__ void log_phase(Ctl *ctl, PhaseLog &lg, int kind, unsigned size)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        const int i = ctl->nphase;
+        const int i = lg.nphase;
         if (i < kMaxTrace) {
             ctl->ph_kind[i] = (unsigned char)kind;
             ctl->ph_size[i] = size;
             ctl->ph_end_ns[i] = globaltimer();
-            ctl->ph_scanned[i] = *(volatile unsigned long long *)&ctl->edges_scanned;
+            ctl->ph_scanned[i] = lg.scanned;
         }
         ctl->nphase = i + 1;
+        ctl->edges_scanned = lg.scanned;
     }
+    lg.nphase++;
 }
 
 // Warp-aggregated append: lanes with flag set write val to arr[base + k],
@@ -339,12 +375,15 @@ __device__ void expand_chunks(const TravArgs &a, unsigned nchunks, const Vis &vi
 }
 
 // ------------------------------------------------------- result write-back
+// kDist: the results are SSSP packed distances (dist), else BFS levels (value).
+template <bool kDist = false>
 __device__ void write_back(const TravArgs &a)
 {
     if (!a.out) return;
     const int gtid = blockIdx.x * kBlock + threadIdx.x, nth = gridDim.x * kBlock;
     for (int v = gtid; v < a.V; v += nth) {
-        unsigned x = __ldcg(&a.value[__ldg(&a.new_of_old[v])]);
+        const int r = __ldg(&a.new_of_old[v]);
+        const unsigned x = kDist ? (unsigned)(__ldcg(&a.dist[r]) >> 32) : __ldcg(&a.value[r]);
         if (a.out_kind == 0) reinterpret_cast<int32_t *>(a.out)[v] = (int32_t)x;
         else if (a.out_kind == 1) reinterpret_cast<unsigned *>(a.out)[v] = x;
         else if (a.out_kind == 2) reinterpret_cast<unsigned char *>(a.out)[v] = (int32_t)x >= 0 ? 1 : 0;
@@ -545,7 +584,7 @@ __device__ void finish_phase(Pusher &p, CtaCounters &cc)
     if (threadIdx.x == 0) {
         Slot *sl = p.o->slot;
         if (cc.mf) atomicAdd(&sl->mf, cc.mf);
-        if (cc.scanned) atomicAdd(&p.a->ctl->edges_scanned, cc.scanned);
+        if (cc.scanned) atomicAdd(&sl->scanned, cc.scanned);
         if (cc.big_total[0]) atomicAdd(&sl->big_add, cc.big_total[0]);
         if (cc.big_total[1]) atomicAdd(&sl->hbig_add, cc.big_total[1]);
         if (cc.far_key) atomicMax(&sl->min_far_bits, cc.far_key);
@@ -694,25 +733,44 @@ struct BfsPush {
     }
 };
 
-// SSSP relaxation.  An improvement below the bucket bound puts the vertex on
-// the next frontier (its light prefix, deduplicated by stamp_near) and, when
-// it has heavy edges, on the heavy list of the current round (deduplicated by
-// stamp_heavy); one at or above the bound goes to the far pile.
+// Packed SSSP distance: float bits in the high word, row-class flags below.
+// Distances are >= +0, so the unsigned order of the words is the float order.
+__device__ __forceinline__ float dist_of(unsigned long long x) { return __uint_as_float((unsigned)(x >> 32)); }
+
+__device__ __forceinline__ unsigned long long pack_dist(float d, unsigned cls)
+{
+    return (static_cast<unsigned long long>(__float_as_uint(d)) << 32) | cls;
+}
+
+// Sets v's bit; true when this call set it.
+__device__ __forceinline__ bool test_and_set(unsigned *bm, int v)
+{
+    const unsigned bit = 1u << (v & 31);
+    return (atomicOr(&bm[v >> 5], bit) & bit) == 0u;
+}
+
+// SSSP relaxation.  A distance is one 64-bit word: the float bits above the
+// row-class flags, so the atomicMin that lowers it leaves the flags intact and
+// the push needs no further load.  An improvement below the bucket bound puts
+// the vertex on the next frontier (light prefix) and, when it has heavy edges,
+// on the heavy list of the current round; one at or above the bound goes to the
+// far pile.  Each of those buffers has a bitmap with a bit per vertex already
+// in it: the push that sets the bit appends the vertex.
 struct SsspPush {
     const TravArgs *a;
-    float thr;          // bucket upper bound (exclusive)
-    int near_id;        // stamp of the frontier being filled
-    int heavy_id;       // stamp of the heavy list being filled
-    int far_id;         // stamp of the current far epoch
+    float thr;               // bucket upper bound (exclusive)
+    unsigned *bm_near;       // bitmap of the frontier being filled
+    unsigned *bm_heavy;      // bitmap of the heavy list being filled
+    unsigned *bm_far;        // bitmap of the far pile being filled
 
-    __device__ __forceinline__ float begin(int u) const { return __uint_as_float(__ldcg(&a->value[u])); }
+    __device__ __forceinline__ float begin(int u) const { return dist_of(__ldcg(&a->dist[u])); }
 
     __device__ __forceinline__ void visit_batch(const int (&)[kBatch], const float (&du)[kBatch],
                                                 const int (&e)[kBatch], const bool (&ok)[kBatch], Pusher &p) const
     {
         int v[kBatch];
         float nd[kBatch];
-        unsigned cur[kBatch];
+        unsigned long long cur[kBatch];
 #pragma unroll
         for (int j = 0; j < kBatch; j++) {
             v[j] = 0;
@@ -723,24 +781,15 @@ struct SsspPush {
             }
         }
 #pragma unroll
-        for (int j = 0; j < kBatch; j++) cur[j] = ok[j] ? __ldcg(&a->value[v[j]]) : 0u;
+        for (int j = 0; j < kBatch; j++) cur[j] = ok[j] ? __ldcg(&a->dist[v[j]]) : 0ull;
         bool imp[kBatch];
 #pragma unroll
         for (int j = 0; j < kBatch; j++) {
             imp[j] = false;
-            if (ok[j] && nd[j] < __uint_as_float(cur[j])) {
-                const int old = atomicMin(reinterpret_cast<int *>(a->value) + v[j], __float_as_int(nd[j]));
-                imp[j] = nd[j] < __int_as_float(old);
-            }
-        }
-        int nl[kBatch], nh[kBatch];
-#pragma unroll
-        for (int j = 0; j < kBatch; j++) {
-            nl[j] = nh[j] = 0;
-            if (imp[j] && nd[j] < thr) {
-                const int deg = __ldg(&a->out_off[v[j] + 1]) - __ldg(&a->out_off[v[j]]);
-                nl[j] = a->nlight ? __ldg(&a->nlight[v[j]]) : deg;
-                nh[j] = deg - nl[j];
+            if (ok[j] && nd[j] < dist_of(cur[j])) {
+                const unsigned long long want = pack_dist(nd[j], (unsigned)cur[j]);
+                const unsigned long long old = atomicMin(&a->dist[v[j]], want);
+                imp[j] = want < old;
             }
         }
         bool light[kBatch], heavy[kBatch], far[kBatch];
@@ -748,18 +797,20 @@ struct SsspPush {
         for (int j = 0; j < kBatch; j++) {
             light[j] = heavy[j] = far[j] = false;
             if (imp[j]) {
+                const unsigned cls = (unsigned)cur[j];
                 if (nd[j] < thr) {
-                    if (nl[j] > 0) light[j] = atomicExch(&a->stamp_near[v[j]], near_id) != near_id;
-                    if (nh[j] > 0) heavy[j] = atomicExch(&a->stamp_heavy[v[j]], heavy_id) != heavy_id;
+                    if (cls & kClsLight) light[j] = test_and_set(bm_near, v[j]);
+                    if (cls & kClsHeavy) heavy[j] = test_and_set(bm_heavy, v[j]);
                 } else {
-                    far[j] = atomicExch(&a->stamp_far[v[j]], far_id) != far_id;
+                    far[j] = test_and_set(bm_far, v[j]);
                 }
             }
         }
 #pragma unroll
         for (int j = 0; j < kBatch; j++) {
-            push(p, 0, light[j], v[j], (unsigned)nl[j]);
-            push(p, 1, heavy[j], v[j], (unsigned)nh[j]);
+            const unsigned cls = (unsigned)cur[j];
+            push(p, 0, light[j], v[j], cls & kClsLightBig ? kSmallDeg + 1u : 1u);
+            push(p, 1, heavy[j], v[j], cls & kClsHeavyBig ? kSmallDeg + 1u : 1u);
             push_far(p, far[j], v[j], far[j] ? 0x7fffffff - __float_as_int(nd[j]) : 0);
         }
     }
@@ -778,6 +829,8 @@ __device__ __forceinline__ void init_counters(CtaCounters &cc)
 // --------------------------------------------------------------- BFS kernel
 __global__ void __launch_bounds__(kBlock, 5) bfs_persistent(TravArgs a)
 {
+    __shared__ SlotView s_view;
+    PhaseLog lg;
     __shared__ WarpStage wst[kWarps];
     __shared__ CtaCounters cc;
     __shared__ int s_dir;
@@ -815,7 +868,7 @@ __global__ void __launch_bounds__(kBlock, 5) bfs_persistent(TravArgs a)
             else if (!(nf >= nf_prev || (double)nf > (double)a.V / a.beta)) d = 0;
             const int forced = planned(a, L);
             if (forced >= 0) d = forced;
-            log_decision(ctl, f, d, 0.0f, 0.0f);
+            log_decision(ctl, lg, f, d, 0.0f, 0.0f);
             if (threadIdx.x == 0) s_dir = d;
         }
         __syncthreads();
@@ -834,7 +887,7 @@ __global__ void __launch_bounds__(kBlock, 5) bfs_persistent(TravArgs a)
                 if (lane_id() == 0) (fcur ? a.front1 : a.front0)[w] = m;
             }
             if (!grid_sync(ctl, a.timeout_ns, ph)) return;
-            log_phase(ctl, 2, (unsigned)nf);
+            log_phase(ctl, lg, 2, (unsigned)nf);
             ph++;
         }
         clear_ahead(ctl, ph);
@@ -909,9 +962,10 @@ __global__ void __launch_bounds__(kBlock, 5) bfs_persistent(TravArgs a)
             bu_steps++;
         }
         finish_phase(p, cc);
-        if (!grid_sync(ctl, a.timeout_ns, ph)) return;
-        log_phase(ctl, dir, (unsigned)nf);
-        const SlotView s0 = read_slot(ctl, ph);
+        if (!grid_sync(ctl, a.timeout_ns, ph, &s_view)) return;
+        lg.scanned += s_view.scanned;
+        log_phase(ctl, lg, dir, (unsigned)nf);
+        const SlotView s0 = s_view;
         ph++;
         nq = s0.q_add;
         nch = s0.chunk_add;
@@ -946,8 +1000,38 @@ __global__ void __launch_bounds__(kBlock, 5) bfs_persistent(TravArgs a)
 // delta = +inf is Bellman-Ford over active vertices (every edge light).  Any
 // order of relaxations reaches the same fixpoint bits: fl(x + w) is monotone
 // in x and not below x for w >= 0.
+//
+// Dedupe bitmaps: near[b], heavy[b] and far[b] hold a bit for every vertex in
+// frontier b, heavy list b and far pile b.  The phase that consumes a buffer
+// clears its bitmap (nothing is pushed to that buffer in the same phase), so a
+// buffer that starts empty always starts with a clear bitmap.  Seeds need no
+// bit: the source is never improved, and the active vertices of a
+// Bellman-Ford start are pushed once by the initialisation alone.
+__device__ __forceinline__ unsigned *sssp_bitmap(const TravArgs &a, int which)
+{
+    return a.bmap + (size_t)which * (size_t)bitmap_stride(a.W);
+}
+
+__device__ __forceinline__ void clear_bitmaps(const TravArgs &a, int first, int count)
+{
+    const int gtid = blockIdx.x * kBlock + threadIdx.x, nth = gridDim.x * kBlock;
+    uint4 *p = reinterpret_cast<uint4 *>(sssp_bitmap(a, first));
+    const int n4 = count * (bitmap_stride(a.W) / 4);
+    for (int i = gtid; i < n4; i += nth) p[i] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+__device__ __forceinline__ unsigned row_class(const TravArgs &a, int v)
+{
+    const int deg = __ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v]);
+    const int nl = a.nlight ? __ldg(&a.nlight[v]) : deg, nh = deg - nl;
+    return (nl > 0 ? kClsLight : 0u) | (nl > kSmallDeg ? kClsLightBig : 0u) | (nh > 0 ? kClsHeavy : 0u) |
+           (nh > kSmallDeg ? kClsHeavyBig : 0u);
+}
+
 __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
 {
+    __shared__ SlotView s_view;
+    PhaseLog lg;
     __shared__ WarpStage wst[kWarps];
     __shared__ CtaCounters cc;
     __shared__ float s_delta;
@@ -958,19 +1042,6 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
     const int lpart = a.nlight ? kPartLight : kPartWhole;
     int ph = 0;
     init_counters(cc);
-    // Stamp ids continue across queries so the stamp arrays need no clearing;
-    // every CTA reads the base before the first barrier, thread 0 of CTA 0
-    // advances it after the last one.  Near the int range they are recycled.
-    int first_id = *(volatile int *)a.id_base;
-    if (first_id > (1 << 30)) {
-        for (int v = gtid; v < a.V; v += nth) {
-            a.stamp_near[v] = -1;
-            a.stamp_far[v] = -1;
-            a.stamp_heavy[v] = -1;
-        }
-        first_id = 0;
-    }
-    int near_id = first_id, far_id = first_id, heavy_id = first_id;
     unsigned nq, nch, nbig;                 // current frontier (light parts)
     unsigned hq = 0, hch = 0, hbig = 0;     // heavy list of the current round
     unsigned long long far_len = 0;
@@ -978,9 +1049,10 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
     float thr = a.delta > 0.0f ? a.delta : INFINITY;
     int cur = 0, hcur = 0, fcur = 0;
 
+    clear_bitmaps(a, 0, 6);
     if (a.source >= 0) {
         const int s = a.source;
-        for (int v = gtid; v < a.V; v += nth) a.value[v] = v == s ? 0u : kFltMaxBits;
+        for (int v = gtid; v < a.V; v += nth) a.dist[v] = pack_dist(v == s ? 0.0f : FLT_MAX, row_class(a, v));
         const int2 lp = row_part(a, s, lpart);
         seed_part(s, lp.x, lp.y, a.q0, a.chunks0, nq, nch);
         nbig = nch ? 1u : 0u;
@@ -989,16 +1061,12 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
             seed_part(s, hp.x, hp.y, a.hq0, a.hch0, hq, hch);
             hbig = hch ? 1u : 0u;
         }
-        if (gtid == 0) {
-            a.stamp_near[s] = near_id;
-            a.stamp_heavy[s] = heavy_id;
-        }
         if (!grid_sync(ctl, a.timeout_ns, ph)) return;
         ph++;
         if (gtid == 0) ctl->t0_ns = globaltimer();
     } else {
-        // start from the distances already in `value` (Bellman-Ford entry
-        // point, every edge light): every vertex below FLT_MAX is active.
+        // start from the distance bits in init_bits (Bellman-Ford entry point,
+        // every edge light): every vertex below FLT_MAX is active.
         thr = INFINITY;
         clear_ahead(ctl, ph);
         const FrontierOut out{{a.q0, nullptr}, {a.chunks0, nullptr}, {0u, 0u}, {0u, 0u}, {kPartWhole, kPartWhole},
@@ -1006,14 +1074,19 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
         Pusher p = make_pusher(a, out, mys);
         for (unsigned base = gwarp * 32; base < (unsigned)a.V; base += nwarps * 32) {
             const int v = (int)(base + lane_id());
-            const bool act = v < a.V && __ldcg(&a.value[v]) < kFltMaxBits;
-            if (act) a.stamp_near[v] = near_id;
-            const unsigned deg = act ? (unsigned)(__ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v])) : 0u;
-            push(p, 0, act && deg > 0, v, deg);
+            unsigned bits = kFltMaxBits, cls = 0;
+            if (v < a.V) {
+                bits = __ldg(&a.init_bits[v]);
+                cls = row_class(a, v);
+                a.dist[v] = (static_cast<unsigned long long>(bits) << 32) | cls;
+            }
+            const bool act = bits < kFltMaxBits && (cls & kClsLight);
+            push(p, 0, act, v, cls & kClsLightBig ? kSmallDeg + 1u : 1u);
         }
         finish_phase(p, cc);
-        if (!grid_sync(ctl, a.timeout_ns, ph)) return;
-        const SlotView s0 = read_slot(ctl, ph);
+        if (!grid_sync(ctl, a.timeout_ns, ph, &s_view)) return;
+        lg.scanned += s_view.scanned;
+        const SlotView s0 = s_view;
         nq = s0.q_add;
         nch = s0.chunk_add;
         nbig = s0.big_add;
@@ -1030,6 +1103,7 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
         if (nq + nch > 0) {
             // light round: frontier (cur) -> next frontier (cur^1) + heavy list (hcur, appended)
             clear_ahead(ctl, ph);
+            clear_bitmaps(a, cur, 1);
             const FrontierOut out{{(cur ? a.q0 : a.q1), (hcur ? a.hq1 : a.hq0)},
                                   {(cur ? a.chunks0 : a.chunks1), (hcur ? a.hch1 : a.hch0)},
                                   {0u, hq},
@@ -1039,15 +1113,16 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
                                   (unsigned)far_len,
                                   &ctl->slot[ph % kSlots]};
             Pusher p = make_pusher(a, out, mys);
-            const SsspPush vis{&a, thr, near_id + 1, heavy_id, far_id};
+            const SsspPush vis{&a, thr, sssp_bitmap(a, cur ^ 1), sssp_bitmap(a, 2 + hcur), sssp_bitmap(a, 4 + fcur)};
             if (lpart == kPartLight)
                 expand_frontier<kPartLight>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, p);
             else
                 expand_frontier<kPartWhole>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, p);
             finish_phase(p, cc);
-            if (!grid_sync(ctl, a.timeout_ns, ph)) return;
-            log_phase(ctl, 3, nq + nbig);
-            const SlotView s0 = read_slot(ctl, ph);
+            if (!grid_sync(ctl, a.timeout_ns, ph, &s_view)) return;
+            lg.scanned += s_view.scanned;
+            log_phase(ctl, lg, 3, nq + nbig);
+            const SlotView s0 = s_view;
             ph++;
             if (gtid == 0 && steps < kMaxTrace) ctl->frontier[steps] = nq + nbig;
             nq = s0.q_add;
@@ -1058,12 +1133,12 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
             hbig += s0.hbig_add;
             far_len += s0.far_add;
             min_far = min(min_far, s0.min_far_bits);
-            near_id++;
             cur ^= 1;
             steps++;
         } else if (hq + hch > 0) {
             // heavy round: heavy list (hcur) -> frontier (cur, empty) + next heavy list (hcur^1)
             clear_ahead(ctl, ph);
+            clear_bitmaps(a, 2 + hcur, 1);
             const FrontierOut out{{(cur ? a.q1 : a.q0), (hcur ? a.hq0 : a.hq1)},
                                   {(cur ? a.chunks1 : a.chunks0), (hcur ? a.hch0 : a.hch1)},
                                   {0u, 0u},
@@ -1073,12 +1148,13 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
                                   (unsigned)far_len,
                                   &ctl->slot[ph % kSlots]};
             Pusher p = make_pusher(a, out, mys);
-            const SsspPush vis{&a, thr, near_id, heavy_id + 1, far_id};
+            const SsspPush vis{&a, thr, sssp_bitmap(a, cur), sssp_bitmap(a, 2 + (hcur ^ 1)), sssp_bitmap(a, 4 + fcur)};
             expand_frontier<kPartHeavy>(a, (hcur ? a.hq1 : a.hq0), hq, (hcur ? a.hch1 : a.hch0), hch, vis, p);
             finish_phase(p, cc);
-            if (!grid_sync(ctl, a.timeout_ns, ph)) return;
-            log_phase(ctl, 5, hq + hbig);
-            const SlotView s0 = read_slot(ctl, ph);
+            if (!grid_sync(ctl, a.timeout_ns, ph, &s_view)) return;
+            lg.scanned += s_view.scanned;
+            log_phase(ctl, lg, 5, hq + hbig);
+            const SlotView s0 = s_view;
             ph++;
             nq = s0.q_add;
             nch = s0.chunk_add;
@@ -1088,7 +1164,6 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
             hbig = s0.hbig_add;
             far_len += s0.far_add;
             min_far = min(min_far, s0.min_far_bits);
-            heavy_id++;
             hcur ^= 1;
             steps++;
         } else if (far_len > 0) {
@@ -1102,15 +1177,15 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
                 const float width = a.delta * sssp_width_scale(o);
                 float hi = __fadd_rn(fmaxf(thr, __int_as_float(min_far)), width);
                 if (!(hi > thr)) hi = nextafterf(thr, INFINITY);
-                log_decision(ctl, f, o, thr, hi);
+                log_decision(ctl, lg, f, o, thr, hi);
                 if (threadIdx.x == 0) s_delta = hi;
             }
             __syncthreads();
             const float told = thr;
             thr = s_delta;  // the new bound, computed once above (same inputs in every CTA)
-            far_id++;
             const int32_t *fp = fcur ? a.far1 : a.far0;
             clear_ahead(ctl, ph);
+            clear_bitmaps(a, 4 + fcur, 1);
             // the (empty) frontier and heavy list receive the entries of the new bucket
             const FrontierOut out{{(cur ? a.q1 : a.q0), (hcur ? a.hq1 : a.hq0)},
                                   {(cur ? a.chunks1 : a.chunks0), (hcur ? a.hch1 : a.hch0)},
@@ -1121,30 +1196,29 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
                                   0u,
                                   &ctl->slot[ph % kSlots]};
             Pusher p = make_pusher(a, out, mys);
+            unsigned *bm_near = sssp_bitmap(a, cur), *bm_heavy = sssp_bitmap(a, 2 + hcur);
+            unsigned *bm_far = sssp_bitmap(a, 4 + (fcur ^ 1));
             for (unsigned long long base = (unsigned long long)gwarp * 32; base < far_len;
                  base += (unsigned long long)nwarps * 32) {
                 const unsigned long long i = base + lane_id();
                 const bool valid = i < far_len;
                 const int v = valid ? fp[i] : 0;
-                const float d = valid ? __uint_as_float(__ldcg(&a.value[v])) : 0.0f;
+                const unsigned long long dv = valid ? __ldcg(&a.dist[v]) : 0ull;
+                const float d = dist_of(dv);
+                const unsigned cls = (unsigned)dv;
                 const bool in_bucket = valid && d >= told && d < thr;
-                int nl = 0, nh = 0;
-                if (in_bucket) {
-                    const int deg = __ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v]);
-                    nl = a.nlight ? __ldg(&a.nlight[v]) : deg;
-                    nh = deg - nl;
-                }
-                const bool light = in_bucket && nl > 0 && atomicExch(&a.stamp_near[v], near_id) != near_id;
-                const bool heavy = in_bucket && nh > 0 && atomicExch(&a.stamp_heavy[v], heavy_id) != heavy_id;
-                const bool keep = valid && d >= thr && atomicExch(&a.stamp_far[v], far_id) != far_id;
-                push(p, 0, light, v, (unsigned)nl);
-                push(p, 1, heavy, v, (unsigned)nh);
+                const bool light = in_bucket && (cls & kClsLight) && test_and_set(bm_near, v);
+                const bool heavy = in_bucket && (cls & kClsHeavy) && test_and_set(bm_heavy, v);
+                const bool keep = valid && d >= thr && test_and_set(bm_far, v);
+                push(p, 0, light, v, cls & kClsLightBig ? kSmallDeg + 1u : 1u);
+                push(p, 1, heavy, v, cls & kClsHeavyBig ? kSmallDeg + 1u : 1u);
                 push_far(p, keep, v, keep ? 0x7fffffff - __float_as_int(d) : 0);
             }
             finish_phase(p, cc);
-            if (!grid_sync(ctl, a.timeout_ns, ph)) return;
-            log_phase(ctl, 4, (unsigned)far_len);
-            const SlotView s0 = read_slot(ctl, ph);
+            if (!grid_sync(ctl, a.timeout_ns, ph, &s_view)) return;
+            lg.scanned += s_view.scanned;
+            log_phase(ctl, lg, 4, (unsigned)far_len);
+            const SlotView s0 = s_view;
             ph++;
             nq = s0.q_add;
             nch = s0.chunk_add;
@@ -1164,10 +1238,8 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
         ctl->steps = steps;
         ctl->buckets = buckets;
         ctl->bottom_up_steps = 0;
-        ctl->next_id = max(max(near_id, far_id), heavy_id) + 2;
-        *a.id_base = ctl->next_id;
     }
-    write_back(a);
+    write_back<true>(a);
 }
 
 // Light-prefix length of every row for `delta` (rows are sorted by weight):
@@ -1189,12 +1261,12 @@ __global__ void light_count_kernel(const int32_t *__restrict__ out_off, const fl
 
 // ------------------------------------------------------------- accounting
 // Algorithmic bytes of the query just run (see trav_query_stats).
-__global__ void sssp_bytes_kernel(const unsigned *__restrict__ value, const int32_t *__restrict__ out_off, int32_t V,
-                                  unsigned long long *acc)
+__global__ void sssp_bytes_kernel(const unsigned long long *__restrict__ dist, const int32_t *__restrict__ out_off,
+                                  int32_t V, unsigned long long *acc)
 {
     unsigned long long r = 0, re = 0;
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
-        if (value[v] != kFltMaxBits) {
+        if ((unsigned)(dist[v] >> 32) != kFltMaxBits) {
             r++;
             re += (unsigned long long)(out_off[v + 1] - out_off[v]);
         }
@@ -1268,10 +1340,11 @@ int device_timeout_err(const Ctl &h, const char *what)
 
 // Enqueue one persistent launch: clear its control block, launch
 // cooperatively (all CTAs co-resident, which the grid barrier needs).
-int enqueue_persistent(int kind, TravArgs &args, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1)
+int enqueue_persistent(int kind, TravArgs &args, int ctas, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1)
 {
     int grid = persistent_grid_size(kind);
     if (grid <= 0) return TRAV_ERR_CUDA;
+    if (ctas > 0 && ctas < grid) grid = ctas;
     TRY_CUDA(cudaMemsetAsync(args.ctl, 0, offsetof(Ctl, dirs), st));
     if (ev0) TRY_CUDA(cudaEventRecord(ev0, st));
     void *params[] = {&args};
@@ -1328,7 +1401,7 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
     const int64_t W = (V + 31) / 32;
     ws->V = g.V;
     ws->chunk_cap = V + g.E / kItem + 1;
-    TRY_CUDA(cudaMalloc(&ws->value, sizeof(unsigned) * V));
+    TRY_CUDA(cudaMalloc(&ws->value, sizeof(unsigned long long) * V));
     TRY_CUDA(cudaMalloc(&ws->visited, sizeof(unsigned) * W));
     TRY_CUDA(cudaMalloc(&ws->front[0], sizeof(unsigned) * W));
     TRY_CUDA(cudaMalloc(&ws->front[1], sizeof(unsigned) * W));
@@ -1336,9 +1409,7 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
         TRY_CUDA(cudaMalloc(&ws->queue[i], sizeof(int32_t) * V));
         TRY_CUDA(cudaMalloc(&ws->far[i], sizeof(int32_t) * V));
     }
-    TRY_CUDA(cudaMalloc(&ws->stamp_near, sizeof(int32_t) * V));
-    TRY_CUDA(cudaMalloc(&ws->stamp_far, sizeof(int32_t) * V));
-    TRY_CUDA(cudaMalloc(&ws->stamp_heavy, sizeof(int32_t) * V));
+    TRY_CUDA(cudaMalloc(&ws->bmap, sizeof(unsigned) * 6 * (size_t)bitmap_stride((int32_t)W)));
     TRY_CUDA(cudaMalloc(&ws->nlight, sizeof(int32_t) * V));
     for (int i = 0; i < 2; i++) {
         TRY_CUDA(cudaMalloc(&ws->hq[i], sizeof(int32_t) * V));
@@ -1348,11 +1419,6 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
     TRY_CUDA(cudaMalloc(&ws->chunks[1], sizeof(int2) * ws->chunk_cap));
     TRY_CUDA(cudaMalloc(&ws->ctl, sizeof(Ctl) * (size_t)nqueries));
     ws->ctl_cap = nqueries;
-    TRY_CUDA(cudaMalloc(&ws->id_base, sizeof(int)));
-    TRY_CUDA(cudaMemsetAsync(ws->id_base, 0, sizeof(int), st));
-    TRY_CUDA(cudaMemsetAsync(ws->stamp_near, 0xff, sizeof(int32_t) * V, st));
-    TRY_CUDA(cudaMemsetAsync(ws->stamp_far, 0xff, sizeof(int32_t) * V, st));
-    TRY_CUDA(cudaMemsetAsync(ws->stamp_heavy, 0xff, sizeof(int32_t) * V, st));
     ws->nlight_delta = -1.0f;
     return TRAV_OK;
 }
@@ -1367,9 +1433,7 @@ void workspace_free(Workspace *ws)
         cudaFree(ws->queue[i]);
         cudaFree(ws->far[i]);
     }
-    cudaFree(ws->stamp_near);
-    cudaFree(ws->stamp_far);
-    cudaFree(ws->stamp_heavy);
+    cudaFree(ws->bmap);
     cudaFree(ws->nlight);
     for (int i = 0; i < 2; i++) {
         cudaFree(ws->hq[i]);
@@ -1378,7 +1442,6 @@ void workspace_free(Workspace *ws)
     cudaFree(ws->chunks[0]);
     cudaFree(ws->chunks[1]);
     cudaFree(ws->ctl);
-    cudaFree(ws->id_base);
     cudaFree(ws->plan[0]);
     cudaFree(ws->plan[1]);
     *ws = Workspace{};
@@ -1397,6 +1460,7 @@ static TravArgs make_args(const DevGraph &g, Workspace *ws)
     a.W = (g.V + 31) / 32;
     a.E = g.E;
     a.value = ws->value;
+    a.dist = reinterpret_cast<unsigned long long *>(ws->value);
     a.visited = ws->visited;
     a.front0 = ws->front[0];
     a.front1 = ws->front[1];
@@ -1404,9 +1468,7 @@ static TravArgs make_args(const DevGraph &g, Workspace *ws)
     a.q1 = ws->queue[1];
     a.far0 = ws->far[0];
     a.far1 = ws->far[1];
-    a.stamp_near = ws->stamp_near;
-    a.stamp_far = ws->stamp_far;
-    a.stamp_heavy = ws->stamp_heavy;
+    a.bmap = ws->bmap;
     a.hq0 = ws->hq[0];
     a.hq1 = ws->hq[1];
     a.hch0 = ws->hchunks[0];
@@ -1415,7 +1477,6 @@ static TravArgs make_args(const DevGraph &g, Workspace *ws)
     a.chunks = ws->chunks[0];
     a.chunks0 = ws->chunks[0];
     a.chunks1 = ws->chunks[1];
-    a.id_base = ws->id_base;
     a.timeout_ns = 10ull * 1000000000ull;
     return a;
 }
@@ -1436,7 +1497,7 @@ int launch_bfs(const DevGraph &g, Workspace *ws, int q, int32_t source_new, cons
     a.mlp = mlp;
     a.plan = ws->plan[0];
     a.plan_len = ws->plan_len[0];
-    return enqueue_persistent(0, a, st, ev0, ev1);
+    return enqueue_persistent(0, a, ws->grid[0], st, ev0, ev1);
 }
 
 int launch_sssp(const DevGraph &g, Workspace *ws, int q, int32_t source_new, float delta, const float *mlp,
@@ -1448,6 +1509,12 @@ int launch_sssp(const DevGraph &g, Workspace *ws, int q, int32_t source_new, flo
     a.max_steps = 4 * g.V + 4096;
     a.force_dir = -1;
     a.delta = (delta > 0.0f && std::isfinite(delta)) ? delta : INFINITY;
+    if (source_new < 0) {
+        // start from distance bits gathered into the second queue buffer (read
+        // by the initialisation only); every edge is light there
+        a.delta = INFINITY;
+        a.init_bits = reinterpret_cast<const unsigned *>(ws->queue[1]);
+    }
     if (std::isfinite(a.delta)) {
         if (ws->nlight_delta != a.delta) {  // rows are sorted by weight: count each light prefix once per delta
             int dev = 0, sms = 148;
@@ -1464,7 +1531,7 @@ int launch_sssp(const DevGraph &g, Workspace *ws, int q, int32_t source_new, flo
     a.mlp = mlp;
     a.plan = ws->plan[1];
     a.plan_len = ws->plan_len[1];
-    return enqueue_persistent(1, a, st, ev0, ev1);
+    return enqueue_persistent(1, a, ws->grid[1], st, ev0, ev1);
 }
 
 // Byte accounting of query q, which must be the last query run (its results
@@ -1480,7 +1547,8 @@ int query_bytes(const DevGraph &g, Workspace *ws, int q, int kind, int64_t *byte
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int grid = sms * 8;
     if (kind == 1) {
-        sssp_bytes_kernel<<<grid, 256, 0, st>>>(ws->value, g.out_off, g.V, acc);
+        sssp_bytes_kernel<<<grid, 256, 0, st>>>(reinterpret_cast<const unsigned long long *>(ws->value), g.out_off,
+                                                g.V, acc);
     } else {
         int nsteps = 0;
         TRY_CUDA(cudaMemcpyAsync(&nsteps, &ws->ctl[q].steps, sizeof(int), cudaMemcpyDeviceToHost, st));

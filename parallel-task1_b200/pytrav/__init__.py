@@ -47,7 +47,7 @@ EXPORTS = [
     "trav_bellman_ford_el_f32", "trav_bfs_el", "trav_el_file_read", "trav_el_file_write", "trav_mlp_set",
     "trav_mlp_param_count", "trav_last_error", "trav_version", "trav_last_batch_ms", "trav_graph_set_stream",
     "trav_bfs_csr_noalloc", "trav_last_phase_log", "trav_mlp_loss_grad", "trav_mlp_train", "trav_set_plan",
-    "trav_last_decisions",
+    "trav_last_decisions", "trav_set_grid",
 ]
 
 
@@ -98,6 +98,7 @@ def lib():
         L.trav_el_file_read.argtypes = [C.c_char_p, i32, C.POINTER(i32), C.POINTER(i64), C.POINTER(i32), vp, vp, vp]
         L.trav_el_file_write.argtypes = [C.c_char_p, i32, i32, i64, vp, vp, vp]
         L.trav_mlp_set.argtypes = [vp, i32, vp, i32]
+        L.trav_set_grid.argtypes = [vp, i32, i32, C.POINTER(i32)]
         L.trav_mlp_param_count.argtypes = [i32]
         L.trav_mlp_param_count.restype = i32
         L.trav_last_batch_ms.argtypes = [vp, vp, i32, C.POINTER(i32)]
@@ -255,6 +256,12 @@ class Graph:
                                          edges.ctypes.data, cap, C.byref(n)))
         k = min(n.value, cap)
         return kind[:k].copy(), size[:k].copy(), end[:k].copy(), edges[:k].copy()
+
+    def set_grid(self, kind: int, ctas: int = 0) -> int:
+        """CTAs of later `kind` launches (0 = as many as fit); returns that maximum."""
+        most = C.c_int32(0)
+        _check(lib().trav_set_grid(self._h, kind, ctas, C.byref(most)))
+        return most.value
 
     def set_plan(self, kind: int, plan=None):
         """Force decisions of later queries of `kind` (0 BFS, 1 SSSP); entries of 255 follow the schedule."""

@@ -75,3 +75,19 @@ def test_phase_log_is_consistent(graph):
     assert np.all(np.diff(end) >= 0) and np.all(np.diff(edges) >= 0)
     assert [k for k in kind if k in (0, 1)] == dirs.tolist()  # one top-down / bottom-up phase per step
     assert frontier.tolist() == [int((want_lv == i).sum()) for i in range(len(frontier))]
+
+
+def test_grid_size_keeps_results(graph):
+    g, src, want_lv, want_d = graph
+    most, most_s = g.set_grid(0), g.set_grid(1)
+    assert min(most, most_s) >= 148
+    for ctas in (1, 3, 37, most // 2, most):
+        g.set_grid(0, ctas)
+        g.set_grid(1, min(ctas, most_s))
+        assert np.array_equal(g.bfs([src])[0], want_lv), ctas
+        got = g.sssp([src], delta=0.05)[0]
+        assert np.array_equal(got.view(np.uint32), want_d), ctas
+    with pytest.raises(T.TravError):
+        g.set_grid(0, most + 1)
+    g.set_grid(0, 0)
+    g.set_grid(1, 0)
