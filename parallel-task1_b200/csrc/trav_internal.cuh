@@ -19,14 +19,13 @@ constexpr int kMaxTrace = 4096;   // steps recorded per query
 constexpr int kMaxDec = 1024;     // schedule decisions recorded per query
 constexpr int kDecFeat = 10;      // features per decision (the schedule MLP's input width)
 constexpr int kSlots = 4;         // ring of per-phase counter slots
-// Row-class flags in the low word of an SSSP packed distance: which parts of
-// the vertex's out-row are non-empty and which are longer than kSmallDeg.  They
-// depend only on the graph and delta, so a 64-bit atomicMin keeps them.
+// Row-class flags in the low bits of an SSSP distance word (dist_bits << 32 |
+// round << kClsBits | flags): which parts of the vertex's out-row are non-empty
+// and which are longer than kSmallDeg.  They depend only on the graph and
+// delta, so the 64-bit atomicMin that lowers a distance keeps them.
 constexpr unsigned kClsLight = 1, kClsLightBig = 2, kClsHeavy = 4, kClsHeavyBig = 8;
-
-// Words per SSSP dedupe bitmap: W rounded up to 16 bytes, so each bitmap can
-// be cleared with 16-byte stores.
-__host__ __device__ inline int32_t bitmap_stride(int32_t W) { return (W + 3) & ~3; }
+constexpr unsigned kClsBits = 4, kClsMask = (1u << kClsBits) - 1u;
+constexpr int kMaxRounds = (1 << (32 - kClsBits)) - 1;  // round ids of one SSSP launch must fit the stamp
 
 // Device status codes written to Ctl::err.
 constexpr int kErrTimeout = 1;    // a bounded grid-barrier wait gave up
@@ -98,14 +97,13 @@ struct DevGraph {
 struct Workspace {
     int32_t V = 0;
     int64_t chunk_cap = 0;
-    // V 64-bit words: BFS levels (int32, the first V words) or SSSP packed
-    // distances (float bits << 32 | row-class flags, see kCls*)
+    // V 64-bit words: BFS levels (int32, the first V words) or SSSP distance
+    // words (float bits << 32 | round << kClsBits | row-class flags)
     unsigned int *value = nullptr;
     unsigned int *visited = nullptr;   // W words
     unsigned int *front[2] = {nullptr, nullptr};  // W words each
     int32_t *queue[2] = {nullptr, nullptr};       // V each
     int32_t *far[2] = {nullptr, nullptr};         // V each
-    unsigned int *bmap = nullptr;      // 6 W-word dedupe bitmaps (SSSP): near[2], heavy[2], far[2]
     int32_t *hq[2] = {nullptr, nullptr};  // SSSP heavy lists (short heavy parts), V each
     int2 *hchunks[2] = {nullptr, nullptr};  // SSSP heavy lists (chunk items), chunk_cap each
     int32_t *nlight = nullptr;         // V: out-edges lighter than nlight_delta (rows are sorted by weight)
@@ -132,12 +130,11 @@ struct TravArgs {
     int64_t E;
     // workspace
     unsigned int *value;        // BFS levels
-    unsigned long long *dist;   // SSSP packed distances (same memory as value)
+    unsigned long long *dist;   // SSSP distance words (same memory as value)
     unsigned int *visited;
     unsigned int *front0, *front1;
     int32_t *q0, *q1;
     int32_t *far0, *far1;
-    unsigned int *bmap;       // SSSP dedupe bitmaps: near[2], heavy[2], far[2], W words each
     int32_t *hq0, *hq1;       // SSSP heavy lists
     int2 *hch0, *hch1;
     const int32_t *__restrict__ nlight;  // light-prefix length per vertex; nullptr = every edge is light

@@ -16,6 +16,7 @@
 #include <cfloat>
 #include <climits>
 #include <cmath>
+#include <algorithm>
 #include <cstddef>
 #include <mutex>
 
@@ -733,35 +734,39 @@ struct BfsPush {
     }
 };
 
-// Packed SSSP distance: float bits in the high word, row-class flags below.
-// Distances are >= +0, so the unsigned order of the words is the float order.
+// SSSP distance word: float bits in the high half, the round stamp and the
+// row-class flags in the low half.  Distances are >= +0, so the unsigned order
+// of the words is the order of the distances (ties broken by the stamp).
 __device__ __forceinline__ float dist_of(unsigned long long x) { return __uint_as_float((unsigned)(x >> 32)); }
 
-__device__ __forceinline__ unsigned long long pack_dist(float d, unsigned cls)
+__device__ __forceinline__ unsigned long long pack_dist(float d, unsigned low)
 {
-    return (static_cast<unsigned long long>(__float_as_uint(d)) << 32) | cls;
+    return (static_cast<unsigned long long>(__float_as_uint(d)) << 32) | low;
 }
 
-// Sets v's bit; true when this call set it.
-__device__ __forceinline__ bool test_and_set(unsigned *bm, int v)
-{
-    const unsigned bit = 1u << (v & 31);
-    return (atomicOr(&bm[v >> 5], bit) & bit) == 0u;
-}
-
-// SSSP relaxation.  A distance is one 64-bit word: the float bits above the
-// row-class flags, so the atomicMin that lowers it leaves the flags intact and
-// the push needs no further load.  An improvement below the bucket bound puts
-// the vertex on the next frontier (light prefix) and, when it has heavy edges,
-// on the heavy list of the current round; one at or above the bound goes to the
-// far pile.  Each of those buffers has a bitmap with a bit per vertex already
-// in it: the push that sets the bit appends the vertex.
+// SSSP relaxation.  A distance is one 64-bit word: the float bits, then the
+// id of the round that last lowered it, then the row-class flags:
+//     dist_bits << 32 | round << 4 | flags.
+// The atomicMin that lowers a distance writes the current round and keeps the
+// flags, and its return value tells the thread both whether it improved the
+// vertex and when the vertex was last improved -- which is all the push needs
+// to decide, without another atomic, whether the vertex is already in the
+// buffer it belongs to:
+//   - next frontier (light prefix, this round only): already there when the
+//     old word is from this round and below the bound;
+//   - heavy list (since h_start): already there when the old word is from a
+//     round >= h_start and below the bound;
+//   - far pile (since f_start): already there when the old word is from a
+//     round >= f_start and at or above the bound.
+// Among the threads that lower one vertex in a round, exactly the first one
+// sees an old word from an earlier round (distances only fall, so a vertex
+// below the bound stays below it).
 struct SsspPush {
     const TravArgs *a;
     float thr;               // bucket upper bound (exclusive)
-    unsigned *bm_near;       // bitmap of the frontier being filled
-    unsigned *bm_heavy;      // bitmap of the heavy list being filled
-    unsigned *bm_far;        // bitmap of the far pile being filled
+    unsigned round;          // id of this round (>= 1)
+    unsigned h_start;        // round the current heavy list began in
+    unsigned f_start;        // round the current far pile began in
 
     __device__ __forceinline__ float begin(int u) const { return dist_of(__ldcg(&a->dist[u])); }
 
@@ -782,27 +787,24 @@ struct SsspPush {
         }
 #pragma unroll
         for (int j = 0; j < kBatch; j++) cur[j] = ok[j] ? __ldcg(&a->dist[v[j]]) : 0ull;
-        bool imp[kBatch];
-#pragma unroll
-        for (int j = 0; j < kBatch; j++) {
-            imp[j] = false;
-            if (ok[j] && nd[j] < dist_of(cur[j])) {
-                const unsigned long long want = pack_dist(nd[j], (unsigned)cur[j]);
-                const unsigned long long old = atomicMin(&a->dist[v[j]], want);
-                imp[j] = want < old;
-            }
-        }
         bool light[kBatch], heavy[kBatch], far[kBatch];
 #pragma unroll
         for (int j = 0; j < kBatch; j++) {
             light[j] = heavy[j] = far[j] = false;
-            if (imp[j]) {
-                const unsigned cls = (unsigned)cur[j];
-                if (nd[j] < thr) {
-                    if (cls & kClsLight) light[j] = test_and_set(bm_near, v[j]);
-                    if (cls & kClsHeavy) heavy[j] = test_and_set(bm_heavy, v[j]);
-                } else {
-                    far[j] = test_and_set(bm_far, v[j]);
+            if (ok[j] && nd[j] < dist_of(cur[j])) {
+                const unsigned cls = (unsigned)cur[j] & kClsMask;
+                const unsigned long long old =
+                    atomicMin(&a->dist[v[j]], pack_dist(nd[j], round << kClsBits | cls));
+                const float od = dist_of(old);
+                if (nd[j] < od) {
+                    const unsigned orr = (unsigned)old >> kClsBits;
+                    if (nd[j] < thr) {
+                        const bool seen_below = od < thr;
+                        light[j] = (cls & kClsLight) && !(seen_below && orr >= round);
+                        heavy[j] = (cls & kClsHeavy) && !(seen_below && orr >= h_start);
+                    } else {
+                        far[j] = !(orr >= f_start);  // od > nd >= thr
+                    }
                 }
             }
         }
@@ -1001,25 +1003,12 @@ __global__ void __launch_bounds__(kBlock, 5) bfs_persistent(TravArgs a)
 // order of relaxations reaches the same fixpoint bits: fl(x + w) is monotone
 // in x and not below x for w >= 0.
 //
-// Dedupe bitmaps: near[b], heavy[b] and far[b] hold a bit for every vertex in
-// frontier b, heavy list b and far pile b.  The phase that consumes a buffer
-// clears its bitmap (nothing is pushed to that buffer in the same phase), so a
-// buffer that starts empty always starts with a clear bitmap.  Seeds need no
-// bit: the source is never improved, and the active vertices of a
-// Bellman-Ford start are pushed once by the initialisation alone.
-__device__ __forceinline__ unsigned *sssp_bitmap(const TravArgs &a, int which)
-{
-    return a.bmap + (size_t)which * (size_t)bitmap_stride(a.W);
-}
-
-__device__ __forceinline__ void clear_bitmaps(const TravArgs &a, int first, int count)
-{
-    const int gtid = blockIdx.x * kBlock + threadIdx.x, nth = gridDim.x * kBlock;
-    uint4 *p = reinterpret_cast<uint4 *>(sssp_bitmap(a, first));
-    const int n4 = count * (bitmap_stride(a.W) / 4);
-    for (int i = gtid; i < n4; i += nth) p[i] = make_uint4(0u, 0u, 0u, 0u);
-}
-
+// Pushes are deduplicated by the round stamps of the distance words (see
+// SsspPush): round ids are phase indices, so the initial words (round 0) are
+// older than every buffer.  A bucket opening pushes from the far pile without
+// lowering a distance, so it stamps each vertex it pushes with its own round
+// (an atomicMax that keeps the distance: nothing lowers distances in that
+// phase).
 __device__ __forceinline__ unsigned row_class(const TravArgs &a, int v)
 {
     const int deg = __ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v]);
@@ -1049,7 +1038,7 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
     float thr = a.delta > 0.0f ? a.delta : INFINITY;
     int cur = 0, hcur = 0, fcur = 0;
 
-    clear_bitmaps(a, 0, 6);
+    unsigned h_start = 1, f_start = 1;      // rounds the heavy list / far pile began in
     if (a.source >= 0) {
         const int s = a.source;
         for (int v = gtid; v < a.V; v += nth) a.dist[v] = pack_dist(v == s ? 0.0f : FLT_MAX, row_class(a, v));
@@ -1103,7 +1092,6 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
         if (nq + nch > 0) {
             // light round: frontier (cur) -> next frontier (cur^1) + heavy list (hcur, appended)
             clear_ahead(ctl, ph);
-            clear_bitmaps(a, cur, 1);
             const FrontierOut out{{(cur ? a.q0 : a.q1), (hcur ? a.hq1 : a.hq0)},
                                   {(cur ? a.chunks0 : a.chunks1), (hcur ? a.hch1 : a.hch0)},
                                   {0u, hq},
@@ -1113,7 +1101,7 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
                                   (unsigned)far_len,
                                   &ctl->slot[ph % kSlots]};
             Pusher p = make_pusher(a, out, mys);
-            const SsspPush vis{&a, thr, sssp_bitmap(a, cur ^ 1), sssp_bitmap(a, 2 + hcur), sssp_bitmap(a, 4 + fcur)};
+            const SsspPush vis{&a, thr, (unsigned)ph, h_start, f_start};
             if (lpart == kPartLight)
                 expand_frontier<kPartLight>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, p);
             else
@@ -1138,7 +1126,6 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
         } else if (hq + hch > 0) {
             // heavy round: heavy list (hcur) -> frontier (cur, empty) + next heavy list (hcur^1)
             clear_ahead(ctl, ph);
-            clear_bitmaps(a, 2 + hcur, 1);
             const FrontierOut out{{(cur ? a.q1 : a.q0), (hcur ? a.hq0 : a.hq1)},
                                   {(cur ? a.chunks1 : a.chunks0), (hcur ? a.hch0 : a.hch1)},
                                   {0u, 0u},
@@ -1148,7 +1135,8 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
                                   (unsigned)far_len,
                                   &ctl->slot[ph % kSlots]};
             Pusher p = make_pusher(a, out, mys);
-            const SsspPush vis{&a, thr, sssp_bitmap(a, cur), sssp_bitmap(a, 2 + (hcur ^ 1)), sssp_bitmap(a, 4 + fcur)};
+            h_start = (unsigned)ph;  // the next heavy list begins in this round
+            const SsspPush vis{&a, thr, (unsigned)ph, h_start, f_start};
             expand_frontier<kPartHeavy>(a, (hcur ? a.hq1 : a.hq0), hq, (hcur ? a.hch1 : a.hch0), hch, vis, p);
             finish_phase(p, cc);
             if (!grid_sync(ctl, a.timeout_ns, ph, &s_view)) return;
@@ -1185,7 +1173,6 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
             thr = s_delta;  // the new bound, computed once above (same inputs in every CTA)
             const int32_t *fp = fcur ? a.far1 : a.far0;
             clear_ahead(ctl, ph);
-            clear_bitmaps(a, 4 + fcur, 1);
             // the (empty) frontier and heavy list receive the entries of the new bucket
             const FrontierOut out{{(cur ? a.q1 : a.q0), (hcur ? a.hq1 : a.hq0)},
                                   {(cur ? a.chunks1 : a.chunks0), (hcur ? a.hch1 : a.hch0)},
@@ -1196,8 +1183,8 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
                                   0u,
                                   &ctl->slot[ph % kSlots]};
             Pusher p = make_pusher(a, out, mys);
-            unsigned *bm_near = sssp_bitmap(a, cur), *bm_heavy = sssp_bitmap(a, 2 + hcur);
-            unsigned *bm_far = sssp_bitmap(a, 4 + (fcur ^ 1));
+            const unsigned round = (unsigned)ph;
+            h_start = f_start = round;  // the heavy list and the far pile begin again here
             for (unsigned long long base = (unsigned long long)gwarp * 32; base < far_len;
                  base += (unsigned long long)nwarps * 32) {
                 const unsigned long long i = base + lane_id();
@@ -1207,9 +1194,11 @@ __global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
                 const float d = dist_of(dv);
                 const unsigned cls = (unsigned)dv;
                 const bool in_bucket = valid && d >= told && d < thr;
-                const bool light = in_bucket && (cls & kClsLight) && test_and_set(bm_near, v);
-                const bool heavy = in_bucket && (cls & kClsHeavy) && test_and_set(bm_heavy, v);
-                const bool keep = valid && d >= thr && test_and_set(bm_far, v);
+                // the pile holds each vertex once (see SsspPush), so every entry is pushed on
+                const bool light = in_bucket && (cls & kClsLight);
+                const bool heavy = in_bucket && (cls & kClsHeavy);
+                const bool keep = valid && d >= thr;
+                if (in_bucket || keep) atomicMax(&a.dist[v], pack_dist(d, round << kClsBits | (cls & kClsMask)));
                 push(p, 0, light, v, cls & kClsLightBig ? kSmallDeg + 1u : 1u);
                 push(p, 1, heavy, v, cls & kClsHeavyBig ? kSmallDeg + 1u : 1u);
                 push_far(p, keep, v, keep ? 0x7fffffff - __float_as_int(d) : 0);
@@ -1409,7 +1398,6 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
         TRY_CUDA(cudaMalloc(&ws->queue[i], sizeof(int32_t) * V));
         TRY_CUDA(cudaMalloc(&ws->far[i], sizeof(int32_t) * V));
     }
-    TRY_CUDA(cudaMalloc(&ws->bmap, sizeof(unsigned) * 6 * (size_t)bitmap_stride((int32_t)W)));
     TRY_CUDA(cudaMalloc(&ws->nlight, sizeof(int32_t) * V));
     for (int i = 0; i < 2; i++) {
         TRY_CUDA(cudaMalloc(&ws->hq[i], sizeof(int32_t) * V));
@@ -1433,7 +1421,6 @@ void workspace_free(Workspace *ws)
         cudaFree(ws->queue[i]);
         cudaFree(ws->far[i]);
     }
-    cudaFree(ws->bmap);
     cudaFree(ws->nlight);
     for (int i = 0; i < 2; i++) {
         cudaFree(ws->hq[i]);
@@ -1468,7 +1455,6 @@ static TravArgs make_args(const DevGraph &g, Workspace *ws)
     a.q1 = ws->queue[1];
     a.far0 = ws->far[0];
     a.far1 = ws->far[1];
-    a.bmap = ws->bmap;
     a.hq0 = ws->hq[0];
     a.hq1 = ws->hq[1];
     a.hch0 = ws->hchunks[0];
@@ -1506,7 +1492,7 @@ int launch_sssp(const DevGraph &g, Workspace *ws, int q, int32_t source_new, flo
     TravArgs a = make_args(g, ws);
     a.ctl = ws->ctl + q;
     a.source = source_new;
-    a.max_steps = 4 * g.V + 4096;
+    a.max_steps = (int32_t)std::min<int64_t>(4 * (int64_t)g.V + 4096, kMaxRounds - 2);
     a.force_dir = -1;
     a.delta = (delta > 0.0f && std::isfinite(delta)) ? delta : INFINITY;
     if (source_new < 0) {
