@@ -409,7 +409,29 @@ __device__ void write_back(const TravArgs &a)
 // its rows are the light prefixes, w < delta), target 1 is the SSSP heavy list
 // (rows are the heavy suffixes).  Rows are sorted by weight, so both parts are
 // contiguous: [off[v], off[v] + nlight[v]) and [off[v] + nlight[v], off[v+1]).
-constexpr int kBatch = 4;  // independent edges per lane per round
+// Launch-shape constants, overridable at build time for tuning sweeps.
+#ifndef TRAV_KBATCH_BFS
+#define TRAV_KBATCH_BFS 4
+#endif
+#ifndef TRAV_KBATCH_SSSP
+#define TRAV_KBATCH_SSSP 2
+#endif
+#ifndef TRAV_SSSP_MIN_BLOCKS
+#define TRAV_SSSP_MIN_BLOCKS 4
+#endif
+#ifndef TRAV_BFS_MIN_BLOCKS
+#define TRAV_BFS_MIN_BLOCKS 5
+#endif
+// Flushes run once per 64-128 staged entries.  Out of line they shrink the
+// relaxation loop but force the pusher state into local memory, which costs
+// more (a 1024x1024 grid SSSP took 90 instead of 52 ms).
+#ifndef TRAV_FLUSH_ATTR
+#define TRAV_FLUSH_ATTR __forceinline__
+#endif
+// Independent edges per lane per round of a relaxation loop.  More edges in
+// flight hide more latency but cost registers: SSSP's 64-register budget
+// (4 CTAs per SM) holds 2 without spilling, and 4 took 30% longer at s23.
+constexpr int kBatchBfs = TRAV_KBATCH_BFS, kBatchSssp = TRAV_KBATCH_SSSP;
 // Per-warp buffers: a push adds at most 32 entries to a buffer that held
 // fewer than its flush mark, so mark + 32 entries always fit.
 constexpr int kWQFlush = 128, kWQ = kWQFlush + 32;
@@ -477,7 +499,7 @@ __device__ __forceinline__ Pusher make_pusher(const TravArgs &a, const FrontierO
     return p;
 }
 
-__device__ __forceinline__ void flush_q(Pusher &p, int t)
+__device__ TRAV_FLUSH_ATTR void flush_q(Pusher &p, int t)
 {
     __syncwarp();
     unsigned base = 0;
@@ -488,7 +510,7 @@ __device__ __forceinline__ void flush_q(Pusher &p, int t)
     p.nq[t] = 0;
 }
 
-__device__ __forceinline__ void flush_big(Pusher &p, int t)
+__device__ TRAV_FLUSH_ATTR void flush_big(Pusher &p, int t)
 {
     __syncwarp();
     for (unsigned r = 0; r < p.nbig[t]; r += 32) {
@@ -516,7 +538,7 @@ __device__ __forceinline__ void flush_big(Pusher &p, int t)
     p.nbig[t] = 0;
 }
 
-__device__ __forceinline__ void flush_far(Pusher &p)
+__device__ TRAV_FLUSH_ATTR void flush_far(Pusher &p)
 {
     __syncwarp();
     unsigned base = 0;
@@ -605,6 +627,7 @@ template <int kPart, class Vis>
 __device__ void expand_frontier(const TravArgs &a, const int32_t *q, unsigned nq, const int2 *chunks, unsigned nch,
                                 const Vis &vis, Pusher &p)
 {
+    constexpr int kBatch = Vis::kBatch;
     const int lane = (int)lane_id();
     const unsigned gwarp = (blockIdx.x * kBlock + threadIdx.x) >> 5, nwarps = (gridDim.x * kBlock) >> 5;
     for (unsigned c = gwarp; c < nch; c += nwarps) {
@@ -698,6 +721,7 @@ __device__ __forceinline__ void seed_part(int s, int rb, int re, int32_t *q, int
 // visit_batch() is called by all 32 lanes of a warp together; ok[j] marks
 // the lanes' edges that exist.  begin() returns the per-vertex value used.
 struct BfsPush {
+    static constexpr int kBatch = kBatchBfs;
     const TravArgs *a;
     int level_next;
 
@@ -762,6 +786,7 @@ __device__ __forceinline__ unsigned long long pack_dist(float d, unsigned low)
 // sees an old word from an earlier round (distances only fall, so a vertex
 // below the bound stays below it).
 struct SsspPush {
+    static constexpr int kBatch = kBatchSssp;
     const TravArgs *a;
     float thr;               // bucket upper bound (exclusive)
     unsigned round;          // id of this round (>= 1)
@@ -829,7 +854,7 @@ __device__ __forceinline__ void init_counters(CtaCounters &cc)
 }
 
 // --------------------------------------------------------------- BFS kernel
-__global__ void __launch_bounds__(kBlock, 5) bfs_persistent(TravArgs a)
+__global__ void __launch_bounds__(kBlock, TRAV_BFS_MIN_BLOCKS) bfs_persistent(TravArgs a)
 {
     __shared__ SlotView s_view;
     PhaseLog lg;
@@ -1017,7 +1042,7 @@ __device__ __forceinline__ unsigned row_class(const TravArgs &a, int v)
            (nh > kSmallDeg ? kClsHeavyBig : 0u);
 }
 
-__global__ void __launch_bounds__(kBlock, 4) sssp_persistent(TravArgs a)
+__global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) sssp_persistent(TravArgs a)
 {
     __shared__ SlotView s_view;
     PhaseLog lg;
