@@ -264,6 +264,46 @@ int trav_last_decisions(trav_graph *g, float *x, uint8_t *choice, int32_t *phase
 const char *trav_last_error(void);
 const char *trav_version(void);
 
+/* ----------------------------------------------------------------- batches
+ * Many BFS / SSSP queries over several graphs in one persistent launch.  The
+ * launch is cut into teams of CTAs; each team runs one query at a time and
+ * takes the next one (largest first) when it is done, so graphs of very
+ * different sizes share the GPU.  No counterpart in the reference, which runs
+ * one query per call. */
+typedef struct trav_batch trav_batch;
+
+typedef struct {
+    int32_t graph;    /* index into the batch's graph list */
+    int32_t kind;     /* 0 = BFS (int32 levels, -1 unreached), 1 = SSSP (float distances, FLT_MAX unreached) */
+    int32_t source;   /* vertex id of that graph */
+    float delta;      /* SSSP bucket width; <= 0 or +inf = Bellman-Ford.  BFS: ignored */
+    int32_t schedule; /* TRAV_SCHEDULE_PLAIN, or TRAV_SCHEDULE_LEARNED with the graph's network */
+    void *out;        /* device array of the graph's V results */
+} trav_query;
+
+typedef struct {
+    int32_t team_ctas; /* CTAs per team (256 threads each) */
+    int32_t small_deg; /* rows of at most this many edges expand in warp tiles, 0..1024 */
+    int32_t item;      /* longer rows are cut into items of this many edges, 64..8192 */
+} trav_batch_shape;
+
+/* A batch over n graph handles of one device (the handles stay the caller's
+ * and must outlive the batch).  The shape starts at 16 CTAs per team, 32, 256. */
+int trav_batch_create(trav_graph *const *graphs, int32_t n, trav_batch **out);
+void trav_batch_free(trav_batch *b);
+
+/* Run n queries in one launch and wait for it; *device_ms (may be NULL)
+ * receives the launch's device time. */
+int trav_batch_run(trav_batch *b, const trav_query *queries, int32_t n, float *device_ms);
+
+/* Time candidate shapes on these queries (each run `reps` times, best kept)
+ * and keep the fastest for later runs; *best (may be NULL) receives it. */
+int trav_batch_autotune(trav_batch *b, const trav_query *queries, int32_t n, int32_t reps,
+                        trav_batch_shape *best);
+
+int trav_batch_set_shape(trav_batch *b, const trav_batch_shape *shape);
+int trav_batch_get_shape(const trav_batch *b, trav_batch_shape *shape);
+
 #ifdef __cplusplus
 }
 #endif

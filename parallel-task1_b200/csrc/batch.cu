@@ -1,0 +1,410 @@
+// Batches: many BFS / SSSP queries over several graphs in one persistent
+// launch (C ABI declared in include/trav.h).  The device side is
+// batch_persistent in traverse.cu; this file builds the query descriptors,
+// owns the teams' scratch and runs the autotuner over launch shapes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <map>
+#include <numeric>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "handle.cuh"
+#include "trav_internal.cuh"
+
+using namespace trav;
+
+#define TRY_CUDA(expr)                                      \
+    do {                                                    \
+        cudaError_t _e = (expr);                            \
+        if (_e != cudaSuccess) return cuda_fail(_e, #expr); \
+    } while (0)
+
+#define TRY(expr)                       \
+    do {                                \
+        int _rc = (expr);               \
+        if (_rc != TRAV_OK) return _rc; \
+    } while (0)
+
+struct trav_batch {
+    std::vector<trav_graph *> graphs;
+    int device = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int32_t vmax = 1, wmax = 1;
+    int64_t emax = 0, chunk_cap = 1;
+    // scratch of the teams (grown on demand)
+    int teams_alloc = 0;
+    unsigned char *team_mem = nullptr;
+    size_t team_bytes = 0;
+    TeamWs *d_teams = nullptr;
+    Ctl *ctl = nullptr;
+    // query descriptors of the last run
+    BatchQuery *d_q = nullptr;
+    int q_cap = 0;
+    unsigned *d_next = nullptr;
+    // light-prefix lengths per (graph, delta)
+    std::map<std::pair<int, float>, int32_t *> nlight;
+    trav_batch_shape shape{16, kSmallDeg, kItem};
+};
+
+namespace {
+
+int bad(const char *msg)
+{
+    set_error(msg);
+    return TRAV_ERR_BAD_ARG;
+}
+
+size_t round_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Byte layout of one team's scratch (every array 256-byte aligned).
+struct TeamLayout {
+    size_t value, visited, front0, front1, q[6], chunks[4], total;
+};
+
+TeamLayout team_layout(const trav_batch *b)
+{
+    TeamLayout L{};
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = o;
+        o += round_up(bytes);
+        return at;
+    };
+    L.value = take(sizeof(unsigned long long) * (size_t)b->vmax);
+    L.visited = take(sizeof(unsigned) * (size_t)b->wmax);
+    L.front0 = take(sizeof(unsigned) * (size_t)b->wmax);
+    L.front1 = take(sizeof(unsigned) * (size_t)b->wmax);
+    for (int i = 0; i < 6; i++) L.q[i] = take(sizeof(int32_t) * (size_t)b->vmax);
+    for (int i = 0; i < 4; i++) L.chunks[i] = take(sizeof(int2) * (size_t)b->chunk_cap);
+    L.total = o;
+    return L;
+}
+
+int ensure_teams(trav_batch *b, int teams)
+{
+    if (teams <= b->teams_alloc) return TRAV_OK;
+    TRY_CUDA(cudaStreamSynchronize(b->st));
+    cudaFree(b->team_mem);
+    cudaFree(b->d_teams);
+    cudaFree(b->ctl);
+    b->team_mem = nullptr;
+    b->d_teams = nullptr;
+    b->ctl = nullptr;
+    b->teams_alloc = 0;
+    const TeamLayout L = team_layout(b);
+    b->team_bytes = L.total;
+    TRY_CUDA(cudaMalloc(&b->team_mem, L.total * (size_t)teams));
+    TRY_CUDA(cudaMalloc(&b->d_teams, sizeof(TeamWs) * (size_t)teams));
+    TRY_CUDA(cudaMalloc(&b->ctl, sizeof(Ctl) * (size_t)teams));
+    std::vector<TeamWs> h((size_t)teams);
+    for (int t = 0; t < teams; t++) {
+        unsigned char *m = b->team_mem + L.total * (size_t)t;
+        TeamWs &w = h[(size_t)t];
+        w.value = reinterpret_cast<unsigned *>(m + L.value);
+        w.visited = reinterpret_cast<unsigned *>(m + L.visited);
+        w.front0 = reinterpret_cast<unsigned *>(m + L.front0);
+        w.front1 = reinterpret_cast<unsigned *>(m + L.front1);
+        int32_t *q[6];
+        for (int i = 0; i < 6; i++) q[i] = reinterpret_cast<int32_t *>(m + L.q[i]);
+        w.q0 = q[0];
+        w.q1 = q[1];
+        w.far0 = q[2];
+        w.far1 = q[3];
+        w.hq0 = q[4];
+        w.hq1 = q[5];
+        int2 *c[4];
+        for (int i = 0; i < 4; i++) c[i] = reinterpret_cast<int2 *>(m + L.chunks[i]);
+        w.chunks0 = c[0];
+        w.chunks1 = c[1];
+        w.hch0 = c[2];
+        w.hch1 = c[3];
+        w.ctl = b->ctl + t;
+    }
+    TRY_CUDA(cudaMemcpy(b->d_teams, h.data(), sizeof(TeamWs) * (size_t)teams, cudaMemcpyHostToDevice));
+    b->teams_alloc = teams;
+    return TRAV_OK;
+}
+
+int shape_ok(const trav_batch_shape &s, int most)
+{
+    if (s.team_ctas < 1 || s.team_ctas > most) return bad("team_ctas must lie in [1, the co-resident CTAs]");
+    if (s.small_deg < 0 || s.small_deg > kMaxSmallDeg) return bad("small_deg must lie in [0, 1024]");
+    if (s.item < kMinItem || s.item > kMaxItem) return bad("item must lie in [64, 8192]");
+    return TRAV_OK;
+}
+
+bool finite_delta(float d) { return d > 0.0f && std::isfinite(d); }
+
+// Descriptors in dispatch order: the most edges first (an SSSP query counts
+// as four BFS queries), so the long queries start while the short ones fill
+// the gaps.
+int build_queries(trav_batch *b, const trav_query *qs, int32_t n, std::vector<BatchQuery> *out)
+{
+    std::vector<int32_t> order((size_t)n);
+    std::iota(order.begin(), order.end(), 0);
+    auto cost = [&](int32_t i) {
+        const trav_graph *g = b->graphs[(size_t)qs[i].graph];
+        return (double)(g->g.E + g->g.V) * (qs[i].kind == 1 ? 4.0 : 1.0);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return cost(x) > cost(y); });
+    out->clear();
+    for (int32_t i : order) {
+        const trav_query &q = qs[i];
+        trav_graph *g = b->graphs[(size_t)q.graph];
+        BatchQuery d{};
+        d.out_off = g->g.out_off;
+        d.out_adj = g->g.out_adj;
+        d.out_w = g->g.out_w;
+        d.in_off = g->g.in_off;
+        d.in_adj = g->g.in_adj;
+        d.new_of_old = g->g.new_of_old;
+        d.V = g->g.V;
+        d.E = g->g.E;
+        d.kind = q.kind;
+        d.source = g->new_of_old[(size_t)q.source];
+        d.out = q.out;
+        d.mlp = q.schedule == TRAV_SCHEDULE_LEARNED ? g->mlp[q.kind] : nullptr;
+        d.delta = INFINITY;
+        d.nlight = nullptr;
+        if (q.kind == 1 && finite_delta(q.delta)) {
+            d.delta = q.delta;
+            auto key = std::make_pair(q.graph, q.delta);
+            auto it = b->nlight.find(key);
+            if (it == b->nlight.end()) {
+                int32_t *p = nullptr;
+                TRY_CUDA(cudaMalloc(&p, sizeof(int32_t) * (size_t)std::max<int32_t>(g->g.V, 1)));
+                it = b->nlight.emplace(key, p).first;
+                TRY(count_light(g->g, q.delta, p, b->st));
+            }
+            d.nlight = it->second;
+        }
+        out->push_back(d);
+    }
+    return TRAV_OK;
+}
+
+int check_queries_host(const trav_batch *b, const trav_query *qs, int32_t n)
+{
+    if (n < 0 || (n > 0 && !qs)) return bad("queries must be a host array of n >= 0 entries");
+    for (int32_t i = 0; i < n; i++) {
+        const trav_query &q = qs[i];
+        if (q.graph < 0 || q.graph >= (int32_t)b->graphs.size()) return bad("query graph index out of range");
+        if (q.kind != 0 && q.kind != 1) return bad("query kind must be 0 (BFS) or 1 (SSSP)");
+        const trav_graph *g = b->graphs[(size_t)q.graph];
+        if (q.source < 0 || q.source >= g->g.V) return bad("query source out of range [0, V)");
+        if (!q.out) return bad("query out must be a device array of V results");
+        if (q.schedule != TRAV_SCHEDULE_PLAIN && q.schedule != TRAV_SCHEDULE_LEARNED)
+            return bad("query schedule must be TRAV_SCHEDULE_PLAIN or TRAV_SCHEDULE_LEARNED");
+        if (q.schedule == TRAV_SCHEDULE_LEARNED && !g->mlp[q.kind])
+            return bad("learned schedule asked for a graph without a network (trav_mlp_set)");
+    }
+    return TRAV_OK;
+}
+
+}  // namespace
+
+namespace {
+
+// One launch of the queries already in b->d_q; *ms receives its device time.
+int run_launch(trav_batch *b, int32_t n, const trav_batch_shape &s, float *ms)
+{
+    const int most = persistent_grid_size(2);
+    if (most <= 0) return TRAV_ERR_CUDA;
+    TRY(shape_ok(s, most));
+    const int teams = std::max(1, std::min(most / s.team_ctas, (int)n));
+    TRY(ensure_teams(b, teams));
+    for (int t = 0; t < teams; t++) TRY_CUDA(cudaMemsetAsync(b->ctl + t, 0, offsetof(Ctl, dirs), b->st));
+    BatchArgs a{};
+    a.queries = b->d_q;
+    a.nq = n;
+    a.next = b->d_next;
+    a.teams = b->d_teams;
+    a.team_ctas = s.team_ctas;
+    a.small_deg = s.small_deg;
+    a.item = s.item;
+    a.timeout_ns = 10ull * 1000000000ull;
+    TRY(launch_batch(a, teams, b->st, b->ev0, b->ev1));
+    TRY_CUDA(cudaStreamSynchronize(b->st));
+    TRY(check_ctls(b->ctl, teams, "batch"));
+    float t = 0.0f;
+    TRY_CUDA(cudaEventElapsedTime(&t, b->ev0, b->ev1));
+    if (ms) *ms = t;
+    return TRAV_OK;
+}
+
+int upload_queries(trav_batch *b, const trav_query *qs, int32_t n)
+{
+    TRY(check_queries_host(b, qs, n));
+    std::vector<BatchQuery> d;
+    TRY(build_queries(b, qs, n, &d));
+    if (n > b->q_cap) {
+        TRY_CUDA(cudaStreamSynchronize(b->st));
+        cudaFree(b->d_q);
+        b->d_q = nullptr;
+        b->q_cap = 0;
+        TRY_CUDA(cudaMalloc(&b->d_q, sizeof(BatchQuery) * (size_t)n));
+        b->q_cap = n;
+    }
+    if (n > 0) TRY_CUDA(cudaMemcpyAsync(b->d_q, d.data(), sizeof(BatchQuery) * (size_t)n, cudaMemcpyHostToDevice, b->st));
+    TRY_CUDA(cudaStreamSynchronize(b->st));  // the host vector goes out of scope
+    return TRAV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int trav_batch_create(trav_graph *const *graphs, int32_t n, trav_batch **out)
+{
+    if (!out) return bad("out must not be NULL");
+    *out = nullptr;
+    if (!graphs || n < 1) return bad("graphs must hold n >= 1 graph handles");
+    for (int32_t i = 0; i < n; i++)
+        if (!graphs[i]) return bad("graph handle is NULL");
+    for (int32_t i = 1; i < n; i++)
+        if (graphs[i]->device != graphs[0]->device) return bad("the graphs of a batch must live on one device");
+    trav_batch *b = new (std::nothrow) trav_batch();
+    if (!b) {
+        set_error("host allocation failed");
+        return TRAV_ERR_OOM;
+    }
+    b->graphs.assign(graphs, graphs + n);
+    b->device = graphs[0]->device;
+    for (const trav_graph *g : b->graphs) {
+        b->vmax = std::max(b->vmax, g->g.V);
+        b->emax = std::max(b->emax, g->g.E);
+    }
+    b->wmax = (b->vmax + 31) / 32;
+    b->chunk_cap = (int64_t)b->vmax + b->emax / kMinItem + 1;
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_next, sizeof(unsigned));
+    if (e != cudaSuccess) {
+        trav_batch_free(b);
+        return cuda_fail(e, "trav_batch_create");
+    }
+    *out = b;
+    return TRAV_OK;
+}
+
+void trav_batch_free(trav_batch *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->st) cudaStreamSynchronize(b->st);
+    cudaFree(b->team_mem);
+    cudaFree(b->d_teams);
+    cudaFree(b->ctl);
+    cudaFree(b->d_q);
+    cudaFree(b->d_next);
+    for (auto &kv : b->nlight) cudaFree(kv.second);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+}
+
+int trav_batch_run(trav_batch *b, const trav_query *queries, int32_t n, float *device_ms)
+{
+    if (!b) return bad("batch handle is NULL");
+    TRY_CUDA(cudaSetDevice(b->device));
+    // the graphs' own streams may still be writing them
+    for (trav_graph *g : b->graphs) TRY_CUDA(cudaStreamSynchronize(g->st));
+    TRY(upload_queries(b, queries, n));
+    if (n == 0) {
+        if (device_ms) *device_ms = 0.0f;
+        return TRAV_OK;
+    }
+    return run_launch(b, n, b->shape, device_ms);
+}
+
+int trav_batch_autotune(trav_batch *b, const trav_query *queries, int32_t n, int32_t reps, trav_batch_shape *best)
+{
+    if (!b) return bad("batch handle is NULL");
+    if (reps < 1) return bad("reps must be >= 1");
+    TRY_CUDA(cudaSetDevice(b->device));
+    for (trav_graph *g : b->graphs) TRY_CUDA(cudaStreamSynchronize(g->st));
+    TRY(upload_queries(b, queries, n));
+    const int most = persistent_grid_size(2);
+    if (most <= 0) return TRAV_ERR_CUDA;
+    if (n > 0) {
+        auto time_of = [&](const trav_batch_shape &s, float *t) {
+            float m = INFINITY;
+            for (int r = 0; r < reps; r++) {
+                float x = 0.0f;
+                TRY(run_launch(b, n, s, &x));
+                m = std::min(m, x);
+            }
+            *t = m;
+            return TRAV_OK;
+        };
+        // coordinate descent: team size, then tile threshold, then item size, twice
+        std::vector<int> team_opts;
+        for (int c : {1, 2, 4, 8, 16, 37, 74, 148, 296})
+            if (c < most) team_opts.push_back(c);
+        team_opts.push_back(most);
+        const int deg_opts[] = {8, 16, 32, 64};
+        const int item_opts[] = {128, 256, 512, 1024};
+        trav_batch_shape cur = b->shape;
+        cur.team_ctas = std::min(cur.team_ctas, most);
+        float cur_t = 0.0f;
+        TRY(time_of(cur, &cur_t));
+        auto consider = [&](trav_batch_shape s) {
+            float t = 0.0f;
+            TRY(time_of(s, &t));
+            if (t < cur_t) {
+                cur = s;
+                cur_t = t;
+            }
+            return TRAV_OK;
+        };
+        for (int pass = 0; pass < 2; pass++) {
+            for (int c : team_opts) {
+                trav_batch_shape s = cur;
+                s.team_ctas = c;
+                TRY(consider(s));
+            }
+            for (int d : deg_opts) {
+                trav_batch_shape s = cur;
+                s.small_deg = d;
+                TRY(consider(s));
+            }
+            for (int it : item_opts) {
+                trav_batch_shape s = cur;
+                s.item = it;
+                TRY(consider(s));
+            }
+        }
+        b->shape = cur;
+    }
+    if (best) *best = b->shape;
+    return TRAV_OK;
+}
+
+int trav_batch_set_shape(trav_batch *b, const trav_batch_shape *shape)
+{
+    if (!b || !shape) return bad("batch handle and shape must not be NULL");
+    TRY_CUDA(cudaSetDevice(b->device));
+    const int most = persistent_grid_size(2);
+    if (most <= 0) return TRAV_ERR_CUDA;
+    TRY(shape_ok(*shape, most));
+    b->shape = *shape;
+    return TRAV_OK;
+}
+
+int trav_batch_get_shape(const trav_batch *b, trav_batch_shape *shape)
+{
+    if (!b || !shape) return bad("batch handle and shape must not be NULL");
+    *shape = b->shape;
+    return TRAV_OK;
+}
+
+}  // extern "C"

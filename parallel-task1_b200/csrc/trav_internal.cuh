@@ -13,8 +13,11 @@ constexpr int kBlock = 256;       // threads per CTA of the persistent kernels
 constexpr int kWarps = kBlock / 32;
 constexpr int kChunk = 512;       // edges per chunk item (two-phase expansion of the allocation-free BFS)
 constexpr int kBigDegree = 512;   // rows longer than this are split into chunks there
-constexpr int kSmallDeg = 32;     // one-phase expansion: rows up to this length go to the CTA-tile queue
-constexpr int kItem = 256;        // one-phase expansion: edges per chunk item of a longer row
+constexpr int kSmallDeg = 32;     // one-phase expansion (default): rows up to this length go to the warp-tile queue
+constexpr int kItem = 256;        // one-phase expansion (default): edges per chunk item of a longer row
+constexpr int kMinItem = 64;      // smallest chunk item a launch may use (sizes the chunk lists)
+constexpr int kMaxItem = 8192;
+constexpr int kMaxSmallDeg = 1024;
 constexpr int kMaxTrace = 4096;   // steps recorded per query
 constexpr int kMaxDec = 1024;     // schedule decisions recorded per query
 constexpr int kDecFeat = 10;      // features per decision (the schedule MLP's input width)
@@ -60,6 +63,7 @@ struct Ctl {
     unsigned long long edges_scanned;  // out-edges expanded (push-side work, all steps)
     int nphase;                   // phases logged below
     int ndec;                     // schedule decisions logged below
+    int cur_query;                // batch launches: the query the team runs next
     unsigned char dirs[kMaxTrace];       // BFS: direction of step s (0 top-down, 1 bottom-up)
     unsigned int frontier[kMaxTrace];    // BFS: frontier size of step s; SSSP: of expansion s
     // phase log (CTA 0, after each grid barrier): kind (0 top-down, 1 bottom-up,
@@ -114,6 +118,8 @@ struct Workspace {
     unsigned char *plan[2] = {nullptr, nullptr};  // forced decisions for BFS / SSSP queries (device)
     int plan_len[2] = {0, 0};
     int grid[2] = {0, 0};              // CTAs of the BFS / SSSP launches (0 = as many as fit)
+    int small_deg = kSmallDeg;         // expansion thresholds of the launches (see TravArgs)
+    int item = kItem;
 };
 
 // Arguments of the persistent kernels (passed by value).
@@ -159,7 +165,48 @@ struct TravArgs {
     const unsigned char *plan;
     int32_t plan_len;
     unsigned long long timeout_ns;
+    // the CTAs that run this query: [cta0, cta0 + ctas) of the launch
+    int32_t cta0, ctas;
+    // expansion thresholds: rows (or row parts) longer than small_deg are cut
+    // into item-edge chunk items, shorter ones go to the warp-tile queue
+    int32_t small_deg, item;
 };
+
+// One query of a batch launch (device descriptor, built by the host).
+struct BatchQuery {
+    const int32_t *out_off, *out_adj, *in_off, *in_adj, *new_of_old;
+    const float *out_w;
+    const int32_t *nlight;  // SSSP light-prefix lengths for delta; nullptr = Bellman-Ford
+    const float *mlp;       // schedule network; nullptr = plain schedule
+    void *out;              // results in original ids: int32 levels (BFS) or float distances (SSSP)
+    int64_t E;
+    int32_t V;
+    int32_t kind;           // 0 = BFS, 1 = SSSP
+    int32_t source;         // new id
+    float delta;            // SSSP bucket width (+inf = Bellman-Ford)
+};
+
+// Scratch of one team of a batch launch, sized for the batch's largest graph.
+struct TeamWs {
+    unsigned int *value;  // 2 * Vmax words
+    unsigned int *visited, *front0, *front1;
+    int32_t *q0, *q1, *far0, *far1, *hq0, *hq1;
+    int2 *chunks0, *chunks1, *hch0, *hch1;
+    Ctl *ctl;
+};
+
+struct BatchArgs {
+    const BatchQuery *queries;  // in dispatch order
+    int32_t nq;
+    unsigned int *next;         // dispatch counter, zero at launch
+    const TeamWs *teams;
+    int32_t team_ctas;          // CTAs per team; the launch has a whole number of teams
+    int32_t small_deg, item;
+    unsigned long long timeout_ns;
+};
+
+__device__ __forceinline__ int team_tid(const TravArgs &a) { return (int)(blockIdx.x - a.cta0) * kBlock + (int)threadIdx.x; }
+__device__ __forceinline__ int team_threads(const TravArgs &a) { return a.ctas * kBlock; }
 
 // ---- host-side helpers (capi.cu) ----
 void set_error(const std::string &msg);
@@ -185,8 +232,13 @@ int launch_sssp(const DevGraph &g, Workspace *ws, int q, int32_t source_new, flo
                 void *out, int out_kind, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1);
 // After the stream finished: turn the device status of queries [0, n) into a return code.
 int check_queries(Workspace *ws, int n, const char *what);
+int check_ctls(const Ctl *ctl, int n, const char *what);  // the same for n device control blocks
+// Light-prefix length of every row of g for delta (rows are sorted by weight).
+int count_light(const DevGraph &g, float delta, int32_t *nlight, cudaStream_t st);
 int query_bytes(const DevGraph &g, Workspace *ws, int q, int kind, int64_t *bytes, int64_t *reached,
                 int64_t *reached_edges, cudaStream_t st);
-int persistent_grid_size(int kind);
+int persistent_grid_size(int kind);  // kind 2 = the batch kernel
+// Enqueue one batch launch of `teams` teams of b.team_ctas CTAs on st.
+int launch_batch(BatchArgs b, int teams, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1);
 
 }  // namespace trav

@@ -77,14 +77,16 @@ struct SlotView {
 // whole CTA (one coalesced load) and leaves it decoded in shared memory: if
 // every warp read the slot itself, the thousands of requests to one L2 line
 // after each barrier would cost as much as a small phase.
-__device__ bool grid_sync(Ctl *ctl, unsigned long long timeout_ns, int phase, SlotView *view = nullptr)
+__device__ bool grid_sync(const TravArgs &a, int phase, SlotView *view = nullptr)
 {
+    Ctl *ctl = a.ctl;
+    const unsigned long long timeout_ns = a.timeout_ns;
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x < 32) {
         if (threadIdx.x == 0) {
             int ok = 1;
-            const unsigned long long nb = gridDim.x;
+            const unsigned long long nb = (unsigned long long)a.ctas;
             unsigned long long old;
             asm volatile("atom.add.acq_rel.gpu.global.u64 %0, [%1], 1;" : "=l"(old) : "l"(&ctl->bar_count) : "memory");
             const unsigned long long target = (old / nb + 1) * nb;
@@ -154,10 +156,11 @@ __device__ __forceinline__ SlotView read_slot(const Ctl *ctl, int ph)
 }
 
 // At the start of phase ph, slot ph+2 was last read right after phase ph-1's
-// barrier by every CTA, so CTA 0 can clear it for reuse in phase ph+2.
-__device__ __forceinline__ void clear_ahead(Ctl *ctl, int ph)
+// barrier by every CTA, so the first CTA can clear it for reuse in phase ph+2.
+__device__ __forceinline__ void clear_ahead(const TravArgs &a, int ph)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    Ctl *ctl = a.ctl;
+    if ((int)blockIdx.x == a.cta0 && threadIdx.x == 0) {
         Slot *s = &ctl->slot[(ph + 2) % kSlots];
         s->q_add = 0;
         s->far_add = 0;
@@ -184,13 +187,14 @@ __device__ __forceinline__ int planned(const TravArgs &a, int i)
 // adds no load to the step's critical path (every CTA waits for CTA 0 at the
 // next barrier).
 struct PhaseLog {
+    bool leader;                     // thread 0 of the query's first CTA
     int nphase = 0, ndec = 0;
     unsigned long long scanned = 0;  // edges expanded so far (sum of the slots' counts)
 };
 
 __device__ __forceinline__ void log_decision(Ctl *ctl, PhaseLog &lg, const Feat &f, int choice, float lo, float hi)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (lg.leader) {
         const int i = lg.ndec;
         if (i < kMaxDec) {
 #pragma unroll
@@ -208,7 +212,7 @@ __device__ __forceinline__ void log_decision(Ctl *ctl, PhaseLog &lg, const Feat 
 // Phase log entry, written by CTA 0 thread 0 right after a grid barrier.
 __device__ __forceinline__ void log_phase(Ctl *ctl, PhaseLog &lg, int kind, unsigned size)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (lg.leader) {
         const int i = lg.nphase;
         if (i < kMaxTrace) {
             ctl->ph_kind[i] = (unsigned char)kind;
@@ -381,7 +385,7 @@ template <bool kDist = false>
 __device__ void write_back(const TravArgs &a)
 {
     if (!a.out) return;
-    const int gtid = blockIdx.x * kBlock + threadIdx.x, nth = gridDim.x * kBlock;
+    const int gtid = team_tid(a), nth = team_threads(a);
     for (int v = gtid; v < a.V; v += nth) {
         const int r = __ldg(&a.new_of_old[v]);
         const unsigned x = kDist ? (unsigned)(__ldcg(&a.dist[r]) >> 32) : __ldcg(&a.value[r]);
@@ -394,8 +398,8 @@ __device__ void write_back(const TravArgs &a)
 
 // ------------------------------------------------------ one-phase frontier
 // The next frontier is written in two parts while it is discovered: vertices
-// whose row to expand has at most kSmallDeg edges go to a queue that the next
-// step expands in 32-vertex warp tiles; longer rows are cut into kItem-edge
+// whose row to expand has at most small_deg edges go to a queue that the next
+// step expands in 32-vertex warp tiles; longer rows are cut into item-edge
 // items, expanded one warp per item.  Both parts are complete when the step's
 // barrier passes, so a step is one phase and one grid barrier, and the work of
 // long rows is spread over every warp of the grid.
@@ -520,7 +524,7 @@ __device__ TRAV_FLUSH_ATTR void flush_big(Pusher &p, int t)
         if (i < p.nbig[t]) {
             v = p.s->big[t][i];
             part = row_part(*p.a, v, p.o->part[t]);
-            nch = (part.y - part.x + kItem - 1) / kItem;
+            nch = (part.y - part.x + p.a->item - 1) / p.a->item;
         }
         int incl = nch;
 #pragma unroll
@@ -532,7 +536,7 @@ __device__ TRAV_FLUSH_ATTR void flush_big(Pusher &p, int t)
         unsigned base = 0;
         if (lane_id() == 0) base = p.o->cbase[t] + atomicAdd(t ? &p.o->slot->hchunk_add : &p.o->slot->chunk_add, total);
         base = __shfl_sync(kFull, base, 0) + (unsigned)(incl - nch);
-        for (int c = 0; c < nch; c++) p.o->chunks[t][base + c] = make_int2(v, part.x + c * kItem);
+        for (int c = 0; c < nch; c++) p.o->chunks[t][base + c] = make_int2(v, part.x + c * p.a->item);
     }
     __syncwarp();
     p.nbig[t] = 0;
@@ -553,7 +557,7 @@ __device__ TRAV_FLUSH_ATTR void flush_far(Pusher &p)
 // length of the row part the target will expand (tile queue or chunk items).
 __device__ __forceinline__ void push(Pusher &p, int t, bool flag, int v, unsigned len)
 {
-    const bool big = flag && len > (unsigned)kSmallDeg;
+    const bool big = flag && len > (unsigned)p.a->small_deg;
     const bool small = flag && !big;
     const unsigned ms = __ballot_sync(kFull, small), mb = __ballot_sync(kFull, big);
     if (ms) {
@@ -629,11 +633,11 @@ __device__ void expand_frontier(const TravArgs &a, const int32_t *q, unsigned nq
 {
     constexpr int kBatch = Vis::kBatch;
     const int lane = (int)lane_id();
-    const unsigned gwarp = (blockIdx.x * kBlock + threadIdx.x) >> 5, nwarps = (gridDim.x * kBlock) >> 5;
+    const unsigned gwarp = (unsigned)team_tid(a) >> 5, nwarps = (unsigned)team_threads(a) >> 5;
     for (unsigned c = gwarp; c < nch; c += nwarps) {
         const int2 it = chunks[c];
         const int u = it.x, start = it.y;
-        const int end = min(start + kItem, row_part(a, u, kPart).y);
+        const int end = min(start + a.item, row_part(a, u, kPart).y);
         const float du = vis.begin(u);
         if (lane == 0) p.scanned += (unsigned long long)(end - start);
         for (int e0 = start; e0 < end; e0 += 32 * kBatch) {
@@ -703,15 +707,16 @@ __device__ void expand_frontier(const TravArgs &a, const int32_t *q, unsigned nq
 
 // One vertex as a frontier of its own (row part [rb, re)): every CTA computes
 // the counts; the items are written by the first threads of the grid.
-__device__ __forceinline__ void seed_part(int s, int rb, int re, int32_t *q, int2 *chunks, unsigned &nq, unsigned &nch)
+__device__ __forceinline__ void seed_part(const TravArgs &a, int s, int rb, int re, int32_t *q, int2 *chunks,
+                                          unsigned &nq, unsigned &nch)
 {
-    const int gtid = blockIdx.x * kBlock + threadIdx.x, nth = gridDim.x * kBlock;
+    const int gtid = team_tid(a), nth = team_threads(a);
     const int len = re - rb;
     nq = nch = 0;
     if (len <= 0) return;
-    if (len > kSmallDeg) {
-        nch = (unsigned)((len + kItem - 1) / kItem);
-        for (int c = gtid; c < (int)nch; c += nth) chunks[c] = make_int2(s, rb + c * kItem);
+    if (len > a.small_deg) {
+        nch = (unsigned)((len + a.item - 1) / a.item);
+        for (int c = gtid; c < (int)nch; c += nth) chunks[c] = make_int2(s, rb + c * a.item);
     } else {
         nq = 1;
         if (gtid == 0) q[0] = s;
@@ -833,11 +838,12 @@ struct SsspPush {
                 }
             }
         }
+        const unsigned big_len = (unsigned)a->small_deg + 1u;  // any length that classifies as a long row
 #pragma unroll
         for (int j = 0; j < kBatch; j++) {
             const unsigned cls = (unsigned)cur[j];
-            push(p, 0, light[j], v[j], cls & kClsLightBig ? kSmallDeg + 1u : 1u);
-            push(p, 1, heavy[j], v[j], cls & kClsHeavyBig ? kSmallDeg + 1u : 1u);
+            push(p, 0, light[j], v[j], cls & kClsLightBig ? big_len : 1u);
+            push(p, 1, heavy[j], v[j], cls & kClsHeavyBig ? big_len : 1u);
             push_far(p, far[j], v[j], far[j] ? 0x7fffffff - __float_as_int(nd[j]) : 0);
         }
     }
@@ -854,26 +860,41 @@ __device__ __forceinline__ void init_counters(CtaCounters &cc)
 }
 
 // --------------------------------------------------------------- BFS kernel
-__global__ void __launch_bounds__(kBlock, TRAV_BFS_MIN_BLOCKS) bfs_persistent(TravArgs a)
+// Shared memory of one query's CTA (the bodies below run inside the
+// single-query kernels and inside the batch kernel).
+struct QueryShared {
+    WarpStage wst[kWarps];
+    CtaCounters cc;
+    SlotView view;
+    int dir;
+    float bound;
+};
+
+// One query on the CTAs [a.cta0, a.cta0 + a.ctas), starting at phase ph0 of the
+// counter-slot ring.  Returns the next phase index, or -1 when the query failed
+// (the error is in a.ctl->err).
+__device__ __forceinline__ int bfs_query(const TravArgs &a, QueryShared &sh, int ph0)
 {
-    __shared__ SlotView s_view;
+    SlotView &s_view = sh.view;
     PhaseLog lg;
-    __shared__ WarpStage wst[kWarps];
-    __shared__ CtaCounters cc;
-    __shared__ int s_dir;
+    lg.leader = (int)blockIdx.x == a.cta0 && threadIdx.x == 0;
+    WarpStage *wst = sh.wst;
+    CtaCounters &cc = sh.cc;
+    int &s_dir = sh.dir;
     Ctl *ctl = a.ctl;
-    const int gtid = blockIdx.x * kBlock + threadIdx.x, nth = gridDim.x * kBlock;
+    const int gtid = team_tid(a), nth = team_threads(a);
     const unsigned gwarp = gtid >> 5, nwarps = nth >> 5;
     WarpStage *mys = &wst[threadIdx.x >> 5];
     const int s = a.source;
-    int ph = 0;
+    int ph = ph0;
 
     init_counters(cc);
     for (int v = gtid; v < a.V; v += nth) reinterpret_cast<int *>(a.value)[v] = v == s ? 0 : -1;
     for (int w = gtid; w < a.W; w += nth) a.visited[w] = w == (s >> 5) ? 1u << (s & 31) : 0u;
     unsigned nq, nch;
-    seed_part(s, __ldg(&a.out_off[s]), __ldg(&a.out_off[s + 1]), a.q0, a.chunks0, nq, nch);
-    if (!grid_sync(ctl, a.timeout_ns, ph)) return;
+    seed_part(a, s, __ldg(&a.out_off[s]), __ldg(&a.out_off[s + 1]), a.q0, a.chunks0, nq, nch);
+    clear_ahead(a, ph);
+    if (!grid_sync(a, ph)) return -1;
     ph++;
     if (gtid == 0) ctl->t0_ns = globaltimer();
 
@@ -883,7 +904,7 @@ __global__ void __launch_bounds__(kBlock, TRAV_BFS_MIN_BLOCKS) bfs_persistent(Tr
     while (nf > 0) {
         if (L >= a.max_steps) {
             if (gtid == 0) atomicCAS(&ctl->err, 0, kErrBudget);
-            return;
+            return -1;
         }
         // direction for this step (same inputs in every CTA -> same answer)
         if (threadIdx.x < 32) {
@@ -906,18 +927,18 @@ __global__ void __launch_bounds__(kBlock, TRAV_BFS_MIN_BLOCKS) bfs_persistent(Tr
         }
         if (dir == 1 && prev_dir == 0) {
             // frontier bitmap from the levels: bit v = (level[v] == L)
-            clear_ahead(ctl, ph);
+            clear_ahead(a, ph);
             for (unsigned w = gwarp; w < (unsigned)a.W; w += nwarps) {
                 const int v = (int)(w * 32 + lane_id());
                 const bool f = v < a.V && (int)a.value[v] == L;
                 const unsigned m = __ballot_sync(kFull, f);
                 if (lane_id() == 0) (fcur ? a.front1 : a.front0)[w] = m;
             }
-            if (!grid_sync(ctl, a.timeout_ns, ph)) return;
+            if (!grid_sync(a, ph)) return -1;
             log_phase(ctl, lg, 2, (unsigned)nf);
             ph++;
         }
-        clear_ahead(ctl, ph);
+        clear_ahead(a, ph);
         const FrontierOut out{{(cur ? a.q0 : a.q1), nullptr}, {(cur ? a.chunks0 : a.chunks1), nullptr}, {0u, 0u},
                               {0u, 0u}, {kPartWhole, kPartWhole}, nullptr, 0u, &ctl->slot[ph % kSlots]};
         Pusher p = make_pusher(a, out, mys);
@@ -989,7 +1010,7 @@ __global__ void __launch_bounds__(kBlock, TRAV_BFS_MIN_BLOCKS) bfs_persistent(Tr
             bu_steps++;
         }
         finish_phase(p, cc);
-        if (!grid_sync(ctl, a.timeout_ns, ph, &s_view)) return;
+        if (!grid_sync(a, ph, &s_view)) return -1;
         lg.scanned += s_view.scanned;
         log_phase(ctl, lg, dir, (unsigned)nf);
         const SlotView s0 = s_view;
@@ -1010,6 +1031,13 @@ __global__ void __launch_bounds__(kBlock, TRAV_BFS_MIN_BLOCKS) bfs_persistent(Tr
         ctl->buckets = 0;
     }
     write_back(a);
+    return ph;
+}
+
+__global__ void __launch_bounds__(kBlock, TRAV_BFS_MIN_BLOCKS) bfs_persistent(TravArgs a)
+{
+    __shared__ QueryShared sh;
+    bfs_query(a, sh, 0);
 }
 
 // -------------------------------------------------------------- SSSP kernel
@@ -1038,23 +1066,25 @@ __device__ __forceinline__ unsigned row_class(const TravArgs &a, int v)
 {
     const int deg = __ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v]);
     const int nl = a.nlight ? __ldg(&a.nlight[v]) : deg, nh = deg - nl;
-    return (nl > 0 ? kClsLight : 0u) | (nl > kSmallDeg ? kClsLightBig : 0u) | (nh > 0 ? kClsHeavy : 0u) |
-           (nh > kSmallDeg ? kClsHeavyBig : 0u);
+    return (nl > 0 ? kClsLight : 0u) | (nl > a.small_deg ? kClsLightBig : 0u) | (nh > 0 ? kClsHeavy : 0u) |
+           (nh > a.small_deg ? kClsHeavyBig : 0u);
 }
 
-__global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) sssp_persistent(TravArgs a)
+__device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, int ph0)
 {
-    __shared__ SlotView s_view;
+    SlotView &s_view = sh.view;
     PhaseLog lg;
-    __shared__ WarpStage wst[kWarps];
-    __shared__ CtaCounters cc;
-    __shared__ float s_delta;
+    lg.leader = (int)blockIdx.x == a.cta0 && threadIdx.x == 0;
+    WarpStage *wst = sh.wst;
+    CtaCounters &cc = sh.cc;
+    float &s_delta = sh.bound;
     Ctl *ctl = a.ctl;
-    const int gtid = blockIdx.x * kBlock + threadIdx.x, nth = gridDim.x * kBlock;
+    const int gtid = team_tid(a), nth = team_threads(a);
     const unsigned gwarp = gtid >> 5, nwarps = nth >> 5;
     WarpStage *mys = &wst[threadIdx.x >> 5];
     const int lpart = a.nlight ? kPartLight : kPartWhole;
-    int ph = 0;
+    const unsigned big_len = (unsigned)a.small_deg + 1u;  // any length that classifies as a long row
+    int ph = ph0;
     init_counters(cc);
     unsigned nq, nch, nbig;                 // current frontier (light parts)
     unsigned hq = 0, hch = 0, hbig = 0;     // heavy list of the current round
@@ -1068,21 +1098,22 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) sssp_persistent(
         const int s = a.source;
         for (int v = gtid; v < a.V; v += nth) a.dist[v] = pack_dist(v == s ? 0.0f : FLT_MAX, row_class(a, v));
         const int2 lp = row_part(a, s, lpart);
-        seed_part(s, lp.x, lp.y, a.q0, a.chunks0, nq, nch);
+        seed_part(a, s, lp.x, lp.y, a.q0, a.chunks0, nq, nch);
         nbig = nch ? 1u : 0u;
         if (a.nlight) {
             const int2 hp = row_part(a, s, kPartHeavy);
-            seed_part(s, hp.x, hp.y, a.hq0, a.hch0, hq, hch);
+            seed_part(a, s, hp.x, hp.y, a.hq0, a.hch0, hq, hch);
             hbig = hch ? 1u : 0u;
         }
-        if (!grid_sync(ctl, a.timeout_ns, ph)) return;
+        clear_ahead(a, ph);
+        if (!grid_sync(a, ph)) return -1;
         ph++;
         if (gtid == 0) ctl->t0_ns = globaltimer();
     } else {
         // start from the distance bits in init_bits (Bellman-Ford entry point,
         // every edge light): every vertex below FLT_MAX is active.
         thr = INFINITY;
-        clear_ahead(ctl, ph);
+        clear_ahead(a, ph);
         const FrontierOut out{{a.q0, nullptr}, {a.chunks0, nullptr}, {0u, 0u}, {0u, 0u}, {kPartWhole, kPartWhole},
                               nullptr, 0u, &ctl->slot[ph % kSlots]};
         Pusher p = make_pusher(a, out, mys);
@@ -1095,10 +1126,10 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) sssp_persistent(
                 a.dist[v] = (static_cast<unsigned long long>(bits) << 32) | cls;
             }
             const bool act = bits < kFltMaxBits && (cls & kClsLight);
-            push(p, 0, act, v, cls & kClsLightBig ? kSmallDeg + 1u : 1u);
+            push(p, 0, act, v, cls & kClsLightBig ? big_len : 1u);
         }
         finish_phase(p, cc);
-        if (!grid_sync(ctl, a.timeout_ns, ph, &s_view)) return;
+        if (!grid_sync(a, ph, &s_view)) return -1;
         lg.scanned += s_view.scanned;
         const SlotView s0 = s_view;
         nq = s0.q_add;
@@ -1112,11 +1143,11 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) sssp_persistent(
     while (true) {
         if (steps + buckets >= a.max_steps) {
             if (gtid == 0) atomicCAS(&ctl->err, 0, kErrBudget);
-            return;
+            return -1;
         }
         if (nq + nch > 0) {
             // light round: frontier (cur) -> next frontier (cur^1) + heavy list (hcur, appended)
-            clear_ahead(ctl, ph);
+            clear_ahead(a, ph);
             const FrontierOut out{{(cur ? a.q0 : a.q1), (hcur ? a.hq1 : a.hq0)},
                                   {(cur ? a.chunks0 : a.chunks1), (hcur ? a.hch1 : a.hch0)},
                                   {0u, hq},
@@ -1132,7 +1163,7 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) sssp_persistent(
             else
                 expand_frontier<kPartWhole>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, p);
             finish_phase(p, cc);
-            if (!grid_sync(ctl, a.timeout_ns, ph, &s_view)) return;
+            if (!grid_sync(a, ph, &s_view)) return -1;
             lg.scanned += s_view.scanned;
             log_phase(ctl, lg, 3, nq + nbig);
             const SlotView s0 = s_view;
@@ -1150,7 +1181,7 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) sssp_persistent(
             steps++;
         } else if (hq + hch > 0) {
             // heavy round: heavy list (hcur) -> frontier (cur, empty) + next heavy list (hcur^1)
-            clear_ahead(ctl, ph);
+            clear_ahead(a, ph);
             const FrontierOut out{{(cur ? a.q1 : a.q0), (hcur ? a.hq0 : a.hq1)},
                                   {(cur ? a.chunks1 : a.chunks0), (hcur ? a.hch0 : a.hch1)},
                                   {0u, 0u},
@@ -1164,7 +1195,7 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) sssp_persistent(
             const SsspPush vis{&a, thr, (unsigned)ph, h_start, f_start};
             expand_frontier<kPartHeavy>(a, (hcur ? a.hq1 : a.hq0), hq, (hcur ? a.hch1 : a.hch0), hch, vis, p);
             finish_phase(p, cc);
-            if (!grid_sync(ctl, a.timeout_ns, ph, &s_view)) return;
+            if (!grid_sync(a, ph, &s_view)) return -1;
             lg.scanned += s_view.scanned;
             log_phase(ctl, lg, 5, hq + hbig);
             const SlotView s0 = s_view;
@@ -1197,7 +1228,7 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) sssp_persistent(
             const float told = thr;
             thr = s_delta;  // the new bound, computed once above (same inputs in every CTA)
             const int32_t *fp = fcur ? a.far1 : a.far0;
-            clear_ahead(ctl, ph);
+            clear_ahead(a, ph);
             // the (empty) frontier and heavy list receive the entries of the new bucket
             const FrontierOut out{{(cur ? a.q1 : a.q0), (hcur ? a.hq1 : a.hq0)},
                                   {(cur ? a.chunks1 : a.chunks0), (hcur ? a.hch1 : a.hch0)},
@@ -1224,12 +1255,12 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) sssp_persistent(
                 const bool heavy = in_bucket && (cls & kClsHeavy);
                 const bool keep = valid && d >= thr;
                 if (in_bucket || keep) atomicMax(&a.dist[v], pack_dist(d, round << kClsBits | (cls & kClsMask)));
-                push(p, 0, light, v, cls & kClsLightBig ? kSmallDeg + 1u : 1u);
-                push(p, 1, heavy, v, cls & kClsHeavyBig ? kSmallDeg + 1u : 1u);
+                push(p, 0, light, v, cls & kClsLightBig ? big_len : 1u);
+                push(p, 1, heavy, v, cls & kClsHeavyBig ? big_len : 1u);
                 push_far(p, keep, v, keep ? 0x7fffffff - __float_as_int(d) : 0);
             }
             finish_phase(p, cc);
-            if (!grid_sync(ctl, a.timeout_ns, ph, &s_view)) return;
+            if (!grid_sync(a, ph, &s_view)) return -1;
             lg.scanned += s_view.scanned;
             log_phase(ctl, lg, 4, (unsigned)far_len);
             const SlotView s0 = s_view;
@@ -1254,6 +1285,96 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) sssp_persistent(
         ctl->bottom_up_steps = 0;
     }
     write_back<true>(a);
+    return ph;
+}
+
+__global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) sssp_persistent(TravArgs a)
+{
+    __shared__ QueryShared sh;
+    sssp_query(a, sh, 0);
+}
+
+// ------------------------------------------------------------ batch kernel
+// Many queries over several graphs in one persistent launch.  The grid is cut
+// into teams of b.team_ctas CTAs; a team runs one query at a time with the
+// same bodies as the single-query kernels (its grid barrier counts only its
+// own CTAs) and then takes the next query from a shared counter, so the
+// queries -- issued largest first -- spread over the teams as they free up.
+// The team's phase index runs on across its queries, so the counter-slot ring
+// stays valid without clearing: every phase clears the slot two ahead.
+__global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) batch_persistent(BatchArgs b)
+{
+    __shared__ QueryShared sh;
+    const int team = (int)blockIdx.x / b.team_ctas;
+    const TeamWs w = b.teams[team];
+    TravArgs t{};
+    t.ctl = w.ctl;
+    t.timeout_ns = b.timeout_ns;
+    t.cta0 = team * b.team_ctas;
+    t.ctas = b.team_ctas;
+    const bool leader = (int)blockIdx.x == t.cta0 && threadIdx.x == 0;
+    int ph = 0;
+    while (true) {
+        // dispatch phase: the team's first thread takes the next query
+        clear_ahead(t, ph);
+        if (leader) w.ctl->cur_query = (int)atomicAdd(b.next, 1u);
+        if (!grid_sync(t, ph)) return;
+        ph++;
+        const int qi = ld_relaxed_int(&w.ctl->cur_query);
+        if (qi >= b.nq) return;
+        const BatchQuery &q = b.queries[qi];
+        TravArgs a = t;
+        a.out_off = q.out_off;
+        a.out_adj = q.out_adj;
+        a.out_w = q.out_w;
+        a.in_off = q.in_off;
+        a.in_adj = q.in_adj;
+        a.new_of_old = q.new_of_old;
+        a.V = q.V;
+        a.W = (q.V + 31) / 32;
+        a.E = q.E;
+        a.value = w.value;
+        a.dist = reinterpret_cast<unsigned long long *>(w.value);
+        a.visited = w.visited;
+        a.front0 = w.front0;
+        a.front1 = w.front1;
+        a.q0 = w.q0;
+        a.q1 = w.q1;
+        a.far0 = w.far0;
+        a.far1 = w.far1;
+        a.hq0 = w.hq0;
+        a.hq1 = w.hq1;
+        a.hch0 = w.hch0;
+        a.hch1 = w.hch1;
+        a.chunks = w.chunks0;
+        a.chunks0 = w.chunks0;
+        a.chunks1 = w.chunks1;
+        a.nlight = q.nlight;
+        a.source = q.source;
+        a.out = q.out;
+        a.mlp = q.mlp;
+        a.plan = nullptr;
+        a.plan_len = 0;
+        a.small_deg = b.small_deg;
+        a.item = b.item;
+        if (q.kind == 0) {
+            a.max_steps = q.V + 1;
+            a.alpha = 15.0f;
+            a.beta = 18.0f;
+            a.force_dir = -1;
+            a.delta = 0.0f;
+            a.out_kind = 0;
+            ph = bfs_query(a, sh, ph);
+        } else {
+            // round stamps are phase indices: the team's whole run must fit them
+            a.max_steps = (int32_t)min((long long)4 * q.V + 4096, (long long)(kMaxRounds - 2 - ph));
+            a.force_dir = -1;
+            a.delta = q.delta;
+            a.out_kind = 1;
+            ph = sssp_query(a, sh, ph);
+        }
+        if (ph < 0) return;
+    }
 }
 
 // Light-prefix length of every row for `delta` (rows are sorted by weight):
@@ -1331,12 +1452,18 @@ __global__ void bfs_bytes_kernel(const int *__restrict__ level, const int32_t *_
     }
 }
 
-int g_grid[2] = {0, 0};
+int g_grid[3] = {0, 0, 0};
 
 #define TRY_CUDA(expr)                                      \
     do {                                                    \
         cudaError_t _e = (expr);                            \
         if (_e != cudaSuccess) return cuda_fail(_e, #expr); \
+    } while (0)
+
+#define TRY(expr)                       \
+    do {                                \
+        int _rc = (expr);               \
+        if (_rc != TRAV_OK) return _rc; \
     } while (0)
 
 int device_timeout_err(const Ctl &h, const char *what)
@@ -1359,6 +1486,8 @@ int enqueue_persistent(int kind, TravArgs &args, int ctas, cudaStream_t st, cuda
     int grid = persistent_grid_size(kind);
     if (grid <= 0) return TRAV_ERR_CUDA;
     if (ctas > 0 && ctas < grid) grid = ctas;
+    args.cta0 = 0;
+    args.ctas = grid;
     TRY_CUDA(cudaMemsetAsync(args.ctl, 0, offsetof(Ctl, dirs), st));
     if (ev0) TRY_CUDA(cudaEventRecord(ev0, st));
     void *params[] = {&args};
@@ -1370,11 +1499,13 @@ int enqueue_persistent(int kind, TravArgs &args, int ctas, cudaStream_t st, cuda
 
 }  // namespace
 
-int check_queries(Workspace *ws, int n, const char *what)
+int check_queries(Workspace *ws, int n, const char *what) { return check_ctls(ws->ctl, n, what); }
+
+int check_ctls(const Ctl *ctl, int n, const char *what)
 {
     for (int q = 0; q < n; q++) {
         Ctl h;
-        TRY_CUDA(cudaMemcpy(&h, ws->ctl + q, offsetof(Ctl, slot), cudaMemcpyDeviceToHost));
+        TRY_CUDA(cudaMemcpy(&h, ctl + q, offsetof(Ctl, slot), cudaMemcpyDeviceToHost));
         int rc = device_timeout_err(h, what);
         if (rc != TRAV_OK) return rc;
     }
@@ -1387,14 +1518,42 @@ int persistent_grid_size(int kind)
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per, kind == 0 ? (const void *)bfs_persistent : (const void *)sssp_persistent, kBlock, 0);
+    const void *fn = kind == 0 ? (const void *)bfs_persistent
+                   : kind == 1 ? (const void *)sssp_persistent : (const void *)batch_persistent;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kBlock, 0);
     if (e != cudaSuccess || per < 1 || sms < 1) {
         cuda_fail(e == cudaSuccess ? cudaErrorInvalidConfiguration : e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
         return -1;
     }
     g_grid[kind] = sms * per;
     return g_grid[kind];
+}
+
+int count_light(const DevGraph &g, float delta, int32_t *nlight, cudaStream_t st)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g.V > 0) light_count_kernel<<<sms * 8, 256, 0, st>>>(g.out_off, g.out_w, g.V, delta, nlight);
+    TRY_CUDA(cudaGetLastError());
+    return TRAV_OK;
+}
+
+int launch_batch(BatchArgs b, int teams, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1)
+{
+    const int most = persistent_grid_size(2);
+    if (most <= 0) return TRAV_ERR_CUDA;
+    if (b.team_ctas < 1 || teams < 1 || (int64_t)teams * b.team_ctas > most) {
+        set_error("batch launch shape exceeds the co-resident CTAs");
+        return TRAV_ERR_BAD_ARG;
+    }
+    TRY_CUDA(cudaMemsetAsync(b.next, 0, sizeof(unsigned), st));
+    if (ev0) TRY_CUDA(cudaEventRecord(ev0, st));
+    void *params[] = {&b};
+    TRY_CUDA(cudaLaunchCooperativeKernel((void *)batch_persistent, dim3(teams * b.team_ctas), dim3(kBlock), params, 0,
+                                         st));
+    if (ev1) TRY_CUDA(cudaEventRecord(ev1, st));
+    return TRAV_OK;
 }
 
 int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_t st)
@@ -1414,7 +1573,7 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
     const int64_t V = g.V > 0 ? g.V : 1;
     const int64_t W = (V + 31) / 32;
     ws->V = g.V;
-    ws->chunk_cap = V + g.E / kItem + 1;
+    ws->chunk_cap = V + g.E / kMinItem + 1;
     TRY_CUDA(cudaMalloc(&ws->value, sizeof(unsigned long long) * V));
     TRY_CUDA(cudaMalloc(&ws->visited, sizeof(unsigned) * W));
     TRY_CUDA(cudaMalloc(&ws->front[0], sizeof(unsigned) * W));
@@ -1489,6 +1648,10 @@ static TravArgs make_args(const DevGraph &g, Workspace *ws)
     a.chunks0 = ws->chunks[0];
     a.chunks1 = ws->chunks[1];
     a.timeout_ns = 10ull * 1000000000ull;
+    a.cta0 = 0;
+    a.ctas = 0;  // set at launch
+    a.small_deg = ws->small_deg;
+    a.item = ws->item;
     return a;
 }
 
@@ -1528,11 +1691,7 @@ int launch_sssp(const DevGraph &g, Workspace *ws, int q, int32_t source_new, flo
     }
     if (std::isfinite(a.delta)) {
         if (ws->nlight_delta != a.delta) {  // rows are sorted by weight: count each light prefix once per delta
-            int dev = 0, sms = 148;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            light_count_kernel<<<sms * 8, 256, 0, st>>>(g.out_off, g.out_w, g.V, a.delta, ws->nlight);
-            TRY_CUDA(cudaGetLastError());
+            TRY(count_light(g, a.delta, ws->nlight, st));
             ws->nlight_delta = a.delta;
         }
         a.nlight = ws->nlight;
@@ -1633,7 +1792,7 @@ __global__ void __launch_bounds__(kBlock) bfs_csr_noalloc_kernel(TravArgs a, int
     for (int v = gtid; v < a.V; v += nth) reinterpret_cast<int *>(a.value)[v] = v == s ? 0 : -1;
     for (int w = gtid; w < a.W; w += nth) a.visited[w] = w == (s >> 5) ? 1u << (s & 31) : 0u;
     if (gtid == 0) a.q0[0] = s;
-    if (!grid_sync(ctl, a.timeout_ns, ph)) return;
+    if (!grid_sync(a, ph)) return;
     ph++;
     unsigned long long qlen = 1;
     int L = 0, cur = 0;
@@ -1644,17 +1803,17 @@ __global__ void __launch_bounds__(kBlock) bfs_csr_noalloc_kernel(TravArgs a, int
         }
         const int32_t *q = cur ? a.q1 : a.q0;
         int32_t *qn = cur ? a.q0 : a.q1;
-        clear_ahead(ctl, ph);
+        clear_ahead(a, ph);
         BfsTopDown vis{&a, L + 1, qn, 0u, &ctl->slot[ph % kSlots]};
         expand_tiles(a, q, (unsigned)qlen, vis, ts, &ctl->slot[ph % kSlots]);
-        if (!grid_sync(ctl, a.timeout_ns, ph)) return;
+        if (!grid_sync(a, ph)) return;
         SlotView s0 = read_slot(ctl, ph);
         ph++;
-        clear_ahead(ctl, ph);
+        clear_ahead(a, ph);
         vis.qbase = s0.q_add;
         vis.slot = &ctl->slot[ph % kSlots];
         expand_chunks(a, s0.chunk_add, vis);
-        if (!grid_sync(ctl, a.timeout_ns, ph)) return;
+        if (!grid_sync(a, ph)) return;
         SlotView s1 = read_slot(ctl, ph);
         ph++;
         qlen = (unsigned long long)s0.q_add + s1.q_add;
@@ -1753,6 +1912,10 @@ extern "C" int trav_bfs_csr_noalloc(const int32_t *row_offsets, const int32_t *a
     a.max_steps = vertices + 1;
     a.force_dir = 0;
     a.timeout_ns = 10ull * 1000000000ull;
+    a.cta0 = 0;
+    a.ctas = sms * per;
+    a.small_deg = kSmallDeg;
+    a.item = kItem;
     void *params[] = {&a, &levels};
     TRY_CUDA(cudaLaunchCooperativeKernel((void *)bfs_csr_noalloc_kernel, dim3(sms * per), dim3(kBlock), params, 0, st));
     TRY_CUDA(cudaStreamSynchronize(st));

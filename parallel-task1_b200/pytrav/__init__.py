@@ -47,7 +47,8 @@ EXPORTS = [
     "trav_bellman_ford_el_f32", "trav_bfs_el", "trav_el_file_read", "trav_el_file_write", "trav_mlp_set",
     "trav_mlp_param_count", "trav_last_error", "trav_version", "trav_last_batch_ms", "trav_graph_set_stream",
     "trav_bfs_csr_noalloc", "trav_last_phase_log", "trav_mlp_loss_grad", "trav_mlp_train", "trav_set_plan",
-    "trav_last_decisions", "trav_set_grid",
+    "trav_last_decisions", "trav_set_grid", "trav_batch_create", "trav_batch_free", "trav_batch_run",
+    "trav_batch_autotune", "trav_batch_set_shape", "trav_batch_get_shape",
 ]
 
 
@@ -63,6 +64,18 @@ class BfsOpts(C.Structure):
 
 class SsspOpts(C.Structure):
     _fields_ = [("schedule", C.c_int32), ("delta", C.c_float)]
+
+
+class Query(C.Structure):
+    _fields_ = [("graph", C.c_int32), ("kind", C.c_int32), ("source", C.c_int32), ("delta", C.c_float),
+                ("schedule", C.c_int32), ("out", C.c_void_p)]
+
+
+class BatchShape(C.Structure):
+    _fields_ = [("team_ctas", C.c_int32), ("small_deg", C.c_int32), ("item", C.c_int32)]
+
+    def as_tuple(self):
+        return (self.team_ctas, self.small_deg, self.item)
 
 
 class QueryStats(C.Structure):
@@ -99,6 +112,13 @@ def lib():
         L.trav_el_file_write.argtypes = [C.c_char_p, i32, i32, i64, vp, vp, vp]
         L.trav_mlp_set.argtypes = [vp, i32, vp, i32]
         L.trav_set_grid.argtypes = [vp, i32, i32, C.POINTER(i32)]
+        L.trav_batch_create.argtypes = [C.POINTER(vp), i32, C.POINTER(vp)]
+        L.trav_batch_free.argtypes = [vp]
+        L.trav_batch_free.restype = None
+        L.trav_batch_run.argtypes = [vp, C.POINTER(Query), i32, C.POINTER(f32)]
+        L.trav_batch_autotune.argtypes = [vp, C.POINTER(Query), i32, i32, C.POINTER(BatchShape)]
+        L.trav_batch_set_shape.argtypes = [vp, C.POINTER(BatchShape)]
+        L.trav_batch_get_shape.argtypes = [vp, C.POINTER(BatchShape)]
         L.trav_mlp_param_count.argtypes = [i32]
         L.trav_mlp_param_count.restype = i32
         L.trav_last_batch_ms.argtypes = [vp, vp, i32, C.POINTER(i32)]
@@ -395,3 +415,64 @@ def write_edges_list(path: str, V: int, src, dst, w, directed: bool = True):
     w = np.ascontiguousarray(w, np.float32)
     _check(lib().trav_el_file_write(path.encode(), int(directed), V, len(src), src.ctypes.data, dst.ctypes.data,
                                     w.ctypes.data))
+
+
+class Batch:
+    """Many BFS / SSSP queries over several graphs in one persistent launch.
+
+    queries: iterable of (graph index, kind 0 BFS / 1 SSSP, source, delta,
+    schedule, out) with `out` a CUDA tensor of the graph's V results (int32
+    levels or float32 distances).
+    """
+
+    def __init__(self, graphs):
+        self.graphs = list(graphs)  # kept alive while the batch exists
+        hs = (C.c_void_p * len(self.graphs))(*[g._h.value for g in self.graphs])
+        h = C.c_void_p()
+        _check(lib().trav_batch_create(hs, len(self.graphs), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            lib().trav_batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _queries(queries):
+        qs = list(queries)
+        arr = (Query * max(1, len(qs)))()
+        for i, (gi, kind, src, delta, sched, out) in enumerate(qs):
+            assert _is_cuda(out), "batch results must be CUDA tensors"
+            arr[i] = Query(gi, kind, int(src), float(delta), sched, _ptr(out))
+        return arr, len(qs)
+
+    def run(self, queries) -> float:
+        """Run the queries in one launch; returns its device time in ms."""
+        arr, n = self._queries(queries)
+        ms = C.c_float(0.0)
+        _check(lib().trav_batch_run(self._h, arr, n, C.byref(ms)))
+        return ms.value
+
+    def autotune(self, queries, reps: int = 2):
+        """Time candidate launch shapes on these queries; keeps and returns the fastest (team_ctas, small_deg, item)."""
+        arr, n = self._queries(queries)
+        best = BatchShape()
+        _check(lib().trav_batch_autotune(self._h, arr, n, reps, C.byref(best)))
+        return best.as_tuple()
+
+    @property
+    def shape(self):
+        s = BatchShape()
+        _check(lib().trav_batch_get_shape(self._h, C.byref(s)))
+        return s.as_tuple()
+
+    @shape.setter
+    def shape(self, value):
+        s = BatchShape(*value)
+        _check(lib().trav_batch_set_shape(self._h, C.byref(s)))

@@ -1,0 +1,139 @@
+"""Batched queries: many BFS / SSSP queries over graphs of uneven sizes in one persistent launch.
+
+Every result of a batch must equal the oracle's (levels, and fp32 distances bit for bit), whatever the launch
+shape the batch runs with; the autotuner may only pick among shapes that all give those results.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import pytrav as T
+
+pytestmark = pytest.mark.gpu
+
+# (scale, edge factor, seed): uneven sizes, like the batched workload's RMAT mix
+GRAPHS = [(8, 8, 3), (12, 16, 4), (10, 32, 5), (13, 8, 6), (9, 24, 7)]
+
+
+@pytest.fixture(scope="module")
+def batch_case():
+    import torch
+
+    assert torch.cuda.is_available()
+    graphs, want = [], []
+    queries = []
+    rng = np.random.default_rng(11)
+    for gi, (scale, ef, seed) in enumerate(GRAPHS):
+        s, d, w = O.rmat(scale, ef, seed=seed)
+        V = 1 << scale
+        g = T.Graph.from_edges(V, s, d, w)
+        graphs.append(g)
+        csr = O.csr(V, s, d, w)
+        deg = np.bincount(s, minlength=V)
+        srcs = rng.choice(np.flatnonzero(deg > 0), 4, replace=False)
+        for k, src in enumerate(srcs):
+            kind = k % 2
+            delta = [0.1, 0.0][(k // 2) % 2] if kind == 1 else 0.0
+            if kind == 0:
+                ref = O.bfs_levels(V, s, d, int(src), csr_arrays=csr)
+                out = torch.empty(V, dtype=torch.int32, device="cuda")
+            else:
+                ref = O.dijkstra(V, s, d, w, int(src), csr_arrays=csr)
+                out = torch.empty(V, dtype=torch.float32, device="cuda")
+            queries.append((gi, kind, int(src), delta, T.SCHEDULE_PLAIN, out))
+            want.append(ref)
+    return graphs, queries, want
+
+
+def _check(queries, want):
+    for (gi, kind, src, delta, _, out), ref in zip(queries, want):
+        got = out.cpu().numpy()
+        if kind == 0:
+            assert np.array_equal(got, ref), (gi, src)
+        else:
+            assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), (gi, src, delta)
+
+
+def _clear(queries):
+    for q in queries:
+        q[5].fill_(7)
+
+
+def test_batch_matches_oracle(batch_case):
+    graphs, queries, want = batch_case
+    b = T.Batch(graphs)
+    _clear(queries)
+    ms = b.run(queries)
+    assert ms > 0
+    _check(queries, want)
+    b.close()
+
+
+@pytest.mark.parametrize("shape", [(1, 32, 256), (3, 8, 64), (37, 64, 1024), (16, 0, 128), (5, 1024, 8192)])
+def test_batch_shapes_keep_results(batch_case, shape):
+    graphs, queries, want = batch_case
+    b = T.Batch(graphs)
+    b.shape = shape
+    assert b.shape == shape
+    _clear(queries)
+    b.run(queries)
+    _check(queries, want)
+    b.close()
+
+
+def test_batch_whole_grid_team_and_repeat(batch_case):
+    graphs, queries, want = batch_case
+    b = T.Batch(graphs)
+    most = graphs[0].set_grid(1)  # the batch kernel has the SSSP kernel's occupancy
+    b.shape = (most, 32, 256)
+    for _ in range(2):
+        _clear(queries)
+        b.run(queries)
+        _check(queries, want)
+    b.close()
+
+
+def test_batch_autotune_picks_a_valid_shape(batch_case):
+    graphs, queries, want = batch_case
+    b = T.Batch(graphs)
+    best = b.autotune(queries, reps=1)
+    assert b.shape == best
+    assert best[0] >= 1 and 0 <= best[1] <= 1024 and 64 <= best[2] <= 8192
+    _clear(queries)
+    b.run(queries)
+    _check(queries, want)
+    b.close()
+
+
+def test_batch_equals_single_query_api(batch_case):
+    graphs, queries, _ = batch_case
+    b = T.Batch(graphs)
+    _clear(queries)
+    b.run(queries)
+    for gi, kind, src, delta, _, out in queries:
+        g = graphs[gi]
+        single = g.bfs([src])[0] if kind == 0 else g.sssp([src], delta=delta)[0]
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), single.view(np.uint32))
+    b.close()
+
+
+def test_batch_errors(batch_case):
+    import torch
+
+    graphs, queries, _ = batch_case
+    b = T.Batch(graphs)
+    out = torch.empty(graphs[0].V, dtype=torch.int32, device="cuda")
+    with pytest.raises(T.TravError):
+        b.run([(len(graphs), 0, 0, 0.0, T.SCHEDULE_PLAIN, out)])
+    with pytest.raises(T.TravError):
+        b.run([(0, 0, graphs[0].V, 0.0, T.SCHEDULE_PLAIN, out)])
+    with pytest.raises(T.TravError):
+        b.run([(0, 2, 0, 0.0, T.SCHEDULE_PLAIN, out)])
+    with pytest.raises(T.TravError):
+        b.run([(0, 0, 0, 0.0, T.SCHEDULE_LEARNED, out)])  # no network installed
+    with pytest.raises(T.TravError):
+        b.shape = (0, 32, 256)
+    with pytest.raises(T.TravError):
+        b.shape = (4, 32, 32)
+    assert b.run([]) == 0.0
+    b.close()
