@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--delta", type=float, default=0.1)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched many-graph measurement")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="target seconds of CPU baseline work")
     return ap.parse_args()
 
@@ -395,10 +396,12 @@ def run_ours(a):
                          "algorithmic_bytes_per_launch": mean_bytes, "mean_launch_ms": mean_ms},
             "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 2 * 4 * n,
                     "d2h_bytes_per_step": 2 * 4 * n * V, "timing": "host clock around synchronous C-ABI calls"},
-            "gpu_launches": traversals * len(runs),
+            "gpu_launches": traversals,
             "ingest_s": ingest_s,
             "clocks": clk,
         }
+        if not a.no_batched and world == 1:
+            line["batched"] = batched_workload(a.seed)
         if not a.no_cpu_baseline and world == 1:
             try:
                 v, desc, cores, _ = cpu_reference_run(a, a.cpu_sample_s)
@@ -412,6 +415,61 @@ def run_ours(a):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def batched_workload(seed: int) -> dict:
+    """The batched workload: 64 seeded RMAT graphs (scale 10-18 and edge factor 8-32 drawn uniformly, the
+    workload's a/b/c/d, weights rand_r/RAND_MAX) with 8 sources each, 512 queries alternating BFS and SSSP
+    (delta 0.1), in one persistent launch with the autotuned shape, against one launch per query through the
+    single-query API.  Results of the two must be identical."""
+    import torch
+
+    import pytrav as T
+
+    rng = np.random.default_rng(seed + 1000)
+    graphs = []
+    for i in range(64):
+        scale, ef = int(rng.integers(10, 19)), int(rng.integers(8, 33))
+        graphs.append(T.Graph.rmat(scale, ef, ABCD, seed=seed + 100 + i, drop_self_loops=True))
+    queries = []
+    for gi, g in enumerate(graphs):
+        deg = g.out_degrees()
+        for k, s in enumerate(rng.choice(np.flatnonzero(deg > 0), 8, replace=False)):
+            kind = k % 2
+            out = torch.empty(g.V, dtype=torch.int32 if kind == 0 else torch.float32, device="cuda")
+            queries.append((gi, kind, int(s), 0.1, T.SCHEDULE_PLAIN, out))
+    edges = sum(graphs[q[0]].E for q in queries)
+    single_ms = 0.0
+    for _ in range(2):  # the second pass is timed (device events of each launch)
+        single_ms = 0.0
+        for gi, kind, s, delta, _, out in queries:
+            g = graphs[gi]
+            if kind == 0:
+                g.bfs([s], out=out.view(1, -1))
+            else:
+                g.sssp([s], out=out.view(1, -1), delta=delta)
+            single_ms += g.last_stats().kernel_ms
+    ref = [q[5].clone() for q in queries]
+    b = T.Batch(graphs)
+    t0 = time.perf_counter()
+    shape = b.autotune(queries, reps=2)
+    tune_s = time.perf_counter() - t0
+    for q in queries:
+        q[5].fill_(7)
+    runs = [b.run(queries) for _ in range(5)]
+    same = all(torch.equal(q[5], r) for q, r in zip(queries, ref))
+    assert same, "batched results differ from the single-query results"
+    ms = statistics.median(runs)
+    b.close()
+    for g in graphs:
+        g.free()
+    return {"workload": "64 RMAT graphs (scale 10-18, edge factor 8-32), 8 sources each: 512 queries, "
+                        "BFS and SSSP (delta 0.1) alternating", "queries": len(queries), "edges_traversed": edges,
+            "ms": ms, "gteps": edges / (ms / 1e3) / 1e9, "shape": {"team_ctas": shape[0], "small_deg": shape[1],
+                                                                 "item": shape[2]},
+            "autotune_s": tune_s, "single_launch_ms": single_ms,
+            "single_launch_gteps": edges / (single_ms / 1e3) / 1e9, "speedup_over_single_launches": single_ms / ms,
+            "identical_results": same, "timing": "device events around the one launch (median of 5)"}
 
 
 def main():

@@ -235,6 +235,13 @@ int trav_mlp_loss_grad(int32_t kind, const float *params, const float *x, const 
 int trav_mlp_train(int32_t kind, float *params, const float *x, const int32_t *labels, int32_t n, int32_t epochs,
                    float lr, float *final_loss);
 
+/* CUDA-graph capture (on != 0): a trav_bfs / trav_sssp call with device
+ * outputs is recorded into a CUDA graph the first time and replayed, with no
+ * per-query launch work on the host, while the call's arguments (sources,
+ * output array, options, launch shape, stream) repeat; any change records a
+ * new graph.  Off by default.  No counterpart in the reference. */
+int trav_graph_set_capture(trav_graph *g, int32_t on);
+
 /* Launch shape of the following queries of one kind on this handle: the
  * persistent kernel runs `ctas` CTAs of 256 threads (1 <= ctas <= the number
  * the device can hold at once, which *max_ctas receives when not NULL);

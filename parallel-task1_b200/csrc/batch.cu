@@ -166,6 +166,7 @@ int build_queries(trav_batch *b, const trav_query *qs, int32_t n, std::vector<Ba
         d.new_of_old = g->g.new_of_old;
         d.V = g->g.V;
         d.E = g->g.E;
+        d.mean_w = g->g.mean_w;
         d.kind = q.kind;
         d.source = g->new_of_old[(size_t)q.source];
         d.out = q.out;

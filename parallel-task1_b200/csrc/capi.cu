@@ -105,6 +105,8 @@ void destroy(trav_graph *h)
         if (h->copied[b]) cudaEventDestroy(h->copied[b]);
     }
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+    for (auto &c : h->cap)
+        if (c.exec) cudaGraphExecDestroy(c.exec);
     cudaFree(h->mlp[0]);
     cudaFree(h->mlp[1]);
     if (h->cst) cudaStreamDestroy(h->cst);
@@ -131,10 +133,41 @@ int new_handle(trav_graph **out)
     return TRAV_OK;
 }
 
+template <class T>
+void put(std::vector<unsigned char> &k, const T &v)
+{
+    const unsigned char *p = reinterpret_cast<const unsigned char *>(&v);
+    k.insert(k.end(), p, p + sizeof(T));
+}
+
+// Everything a captured call's launches depend on besides the graph itself.
+std::vector<unsigned char> capture_key(const trav_graph *g, int kind, const int32_t *sources, int32_t n,
+                                       const trav_bfs_opts *bo, float delta, const float *mlp, const void *out)
+{
+    std::vector<unsigned char> k;
+    put(k, kind);
+    put(k, n);
+    for (int32_t i = 0; i < n; i++) put(k, sources[i]);
+    put(k, out);
+    put(k, mlp);
+    put(k, delta);
+    if (bo) put(k, *bo);
+    put(k, g->ws.grid[kind]);
+    put(k, g->ws.small_deg);
+    put(k, g->ws.item);
+    put(k, g->ws.plan[kind]);
+    put(k, g->ws.plan_len[kind]);
+    put(k, g->st);
+    put(k, g->ws.ctl);
+    return k;
+}
+
 // Run n queries of one kind.  Device outputs go straight to out + q*V; host
 // outputs are written to a double-buffered device staging area and copied on
 // a second stream, so the copy of query q overlaps the traversal of q+1
-// (fully when `out` is pinned host memory).
+// (fully when `out` is pinned host memory).  With capture on, a call with
+// device outputs is recorded into a CUDA graph the first time and replayed
+// while its arguments repeat.
 int run_batch(trav_graph *g, int kind, const int32_t *sources, int32_t n, const trav_bfs_opts *bo, float delta,
               const float *mlp, void *out, int32_t mem)
 {
@@ -147,24 +180,55 @@ int run_batch(trav_graph *g, int kind, const int32_t *sources, int32_t n, const 
     }
     const size_t V = (size_t)g->g.V;
     unsigned char *base = static_cast<unsigned char *>(out);
-    for (int32_t q = 0; q < n; q++) {
-        const int32_t s_new = g->new_of_old[(size_t)sources[q]];
-        void *dst;
-        const int b = q & 1;
-        if (mem == TRAV_MEM_DEVICE) {
-            dst = base + 4 * V * (size_t)q;
-        } else {
-            if (q >= 2) TRY_CUDA(cudaStreamWaitEvent(g->st, g->copied[b], 0));
-            dst = g->staging[b];
+    auto enqueue = [&]() -> int {
+        for (int32_t q = 0; q < n; q++) {
+            const int32_t s_new = g->new_of_old[(size_t)sources[q]];
+            void *dst;
+            const int b = q & 1;
+            if (mem == TRAV_MEM_DEVICE) {
+                dst = base + 4 * V * (size_t)q;
+            } else {
+                if (q >= 2) TRY_CUDA(cudaStreamWaitEvent(g->st, g->copied[b], 0));
+                dst = g->staging[b];
+            }
+            if (kind == 0) TRY(launch_bfs(g->g, &g->ws, q, s_new, *bo, mlp, dst, 0, g->st, g->ev[2 * q], g->ev[2 * q + 1]));
+            else TRY(launch_sssp(g->g, &g->ws, q, s_new, delta, mlp, dst, 1, g->st, g->ev[2 * q], g->ev[2 * q + 1]));
+            if (mem == TRAV_MEM_HOST) {
+                TRY_CUDA(cudaEventRecord(g->done[b], g->st));
+                TRY_CUDA(cudaStreamWaitEvent(g->cst, g->done[b], 0));
+                TRY_CUDA(cudaMemcpyAsync(base + 4 * V * (size_t)q, dst, 4 * V, cudaMemcpyDeviceToHost, g->cst));
+                TRY_CUDA(cudaEventRecord(g->copied[b], g->cst));
+            }
         }
-        if (kind == 0) TRY(launch_bfs(g->g, &g->ws, q, s_new, *bo, mlp, dst, 0, g->st, g->ev[2 * q], g->ev[2 * q + 1]));
-        else TRY(launch_sssp(g->g, &g->ws, q, s_new, delta, mlp, dst, 1, g->st, g->ev[2 * q], g->ev[2 * q + 1]));
-        if (mem == TRAV_MEM_HOST) {
-            TRY_CUDA(cudaEventRecord(g->done[b], g->st));
-            TRY_CUDA(cudaStreamWaitEvent(g->cst, g->done[b], 0));
-            TRY_CUDA(cudaMemcpyAsync(base + 4 * V * (size_t)q, dst, 4 * V, cudaMemcpyDeviceToHost, g->cst));
-            TRY_CUDA(cudaEventRecord(g->copied[b], g->cst));
+        return TRAV_OK;
+    };
+    if (g->capture && mem == TRAV_MEM_DEVICE) {
+        trav_graph::Captured &c = g->cap[kind];
+        std::vector<unsigned char> key = capture_key(g, kind, sources, n, bo, delta, mlp, out);
+        if (!c.exec || c.key != key) {
+            if (c.exec) cudaGraphExecDestroy(c.exec);
+            c.exec = nullptr;
+            c.key.clear();
+            if (kind == 1) g->ws.nlight_delta = -1.0f;  // the graph must count the light prefixes itself
+            TRY_CUDA(cudaStreamBeginCapture(g->st, cudaStreamCaptureModeThreadLocal));
+            const int rc = enqueue();
+            cudaGraph_t graph = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(g->st, &graph);
+            if (rc != TRAV_OK) {
+                if (graph) cudaGraphDestroy(graph);
+                return rc;
+            }
+            if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+            const cudaError_t ei = cudaGraphInstantiate(&c.exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ei != cudaSuccess) return cuda_fail(ei, "cudaGraphInstantiate");
+            c.key = std::move(key);
         }
+        TRY_CUDA(cudaGraphLaunch(c.exec, g->st));
+        // the graph recounts the light prefixes for its own delta
+        if (kind == 1) g->ws.nlight_delta = -1.0f;
+    } else {
+        TRY(enqueue());
     }
     TRY_CUDA(cudaStreamSynchronize(g->st));
     TRY_CUDA(cudaStreamSynchronize(g->cst));
@@ -386,6 +450,20 @@ int trav_graph_set_stream(trav_graph *g, void *stream)
     TRY_CUDA(cudaSetDevice(g->device));
     TRY_CUDA(cudaStreamSynchronize(g->st));
     g->st = stream ? static_cast<cudaStream_t>(stream) : g->own_st;
+    return TRAV_OK;
+}
+
+int trav_graph_set_capture(trav_graph *g, int32_t on)
+{
+    if (!g) return bad("graph handle is NULL");
+    TRY_CUDA(cudaSetDevice(g->device));
+    TRY_CUDA(cudaStreamSynchronize(g->st));
+    g->capture = on != 0;
+    for (auto &c : g->cap) {
+        if (c.exec) cudaGraphExecDestroy(c.exec);
+        c.exec = nullptr;
+        c.key.clear();
+    }
     return TRAV_OK;
 }
 

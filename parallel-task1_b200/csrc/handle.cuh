@@ -22,4 +22,12 @@ struct trav_graph {
     float *mlp[2] = {nullptr, nullptr};  // device MLP parameters: 0 = BFS, 1 = SSSP
     int last_kind = -1;
     int last_n = 0;
+    // CUDA-graph capture of multi-source calls with device outputs: the
+    // launches of a call are captured once and replayed while the call's
+    // arguments repeat (one graph per kind)
+    bool capture = false;
+    struct Captured {
+        cudaGraphExec_t exec = nullptr;
+        std::vector<unsigned char> key;
+    } cap[2];
 };

@@ -182,6 +182,27 @@ int grid_for(int64_t n, int block = 256)
 }
 
 // Scoped device allocation.
+// Sum of the weights in fixed order: each block adds a grid-stride share in
+// double and reduces it in a fixed tree; the host adds the block sums in
+// block order.  (The mean weight is a schedule feature, so it must not vary
+// from run to run.)
+constexpr int kWSumBlocks = 256;
+
+__global__ void weight_sum_kernel(int64_t E, const float *__restrict__ w, double *__restrict__ partial)
+{
+    __shared__ double sh[256];
+    double acc = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (int64_t)gridDim.x * blockDim.x)
+        acc += (double)w[i];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 128; o; o >>= 1) {
+        if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
 template <class T>
 struct DBuf {
     T *p = nullptr;
@@ -351,11 +372,23 @@ int build_graph_device(int32_t V, int64_t E, const int32_t *d_src, const int32_t
     }
     int32_t maxdeg = 0;
     if (V > 0) TRY_CUDA(cudaMemcpyAsync(&maxdeg, deg_sorted.p, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    double wsum = 0.0;
+    if (E > 0) {
+        DBuf<double> part;
+        TRY_CUDA(part.alloc(kWSumBlocks));
+        weight_sum_kernel<<<kWSumBlocks, 256, 0, st>>>(E, out_w.p, part.p);
+        TRY_CUDA(cudaGetLastError());
+        double h[kWSumBlocks];
+        TRY_CUDA(cudaMemcpyAsync(h, part.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+        TRY_CUDA(cudaStreamSynchronize(st));
+        for (int b = 0; b < kWSumBlocks; b++) wsum += h[b];
+    }
     TRY_CUDA(cudaStreamSynchronize(st));
 
     out->V = V;
     out->E = E;
     out->max_out_degree = maxdeg;
+    out->mean_w = E > 0 ? (float)(wsum / (double)E) : 0.0f;
     out->out_off = out_off.release();
     out->out_adj = out_adj.release();
     out->out_w = out_w.release();

@@ -16,12 +16,13 @@ namespace trav {
 constexpr int kFeat = 10;
 constexpr int kHidden = 32;
 constexpr int kBfsOut = 2;      // 0 = top-down (push), 1 = bottom-up (pull)
-constexpr int kSsspOut = 4;     // bucket width = delta * {1, 4, 16, 64} (merge 1, 4, 16, 64 buckets)
+constexpr int kSsspOut = 6;     // bucket width = delta * 4^k, k = 0..5 (merge 1 .. 1024 buckets)
 
 __host__ __device__ constexpr int mlp_param_count(int O)
 {
     return kHidden * kFeat + kHidden + kHidden * kHidden + kHidden + O * kHidden + O;
 }
+constexpr int kMlpMaxParams = kHidden * kFeat + kHidden + kHidden * kHidden + kHidden + kSsspOut * kHidden + kSsspOut;
 
 struct Feat {
     float x[kFeat];
@@ -29,43 +30,56 @@ struct Feat {
 
 __host__ __device__ inline float flog2p1(double v) { return (float)log2(1.0 + (v > 0 ? v : 0)); }
 
-// BFS step features: frontier size, frontier out-edges, unvisited out-edges,
-// previous frontier size, step index, graph size and mean degree, growth,
-// edge ratio and the previous step's direction.
+// sign(v) * log2(1 + |v|): bounded growth for quantities of any scale
+__host__ __device__ inline float fslog2p1(double v) { return v < 0 ? -flog2p1(-v) : flog2p1(v); }
+
+// BFS step features, all scale-free so that graphs larger than the training
+// graphs stay in range: the two ratios Beamer's switch tests (frontier
+// out-edges / unexplored edges, frontier / V), frontier growth, the step
+// index, mean degree, the explored and frontier shares of the edges, whether
+// the frontier grew, the previous direction and the plain switch's own choice
+// (so the network only has to learn where to differ from it).
 __host__ __device__ inline Feat bfs_features(int step, unsigned long long nf, unsigned long long mf,
                                              unsigned long long mu, unsigned long long nf_prev, int V, long long E,
-                                             int prev_dir)
+                                             int prev_dir, int plain_dir)
 {
     Feat f;
-    f.x[0] = flog2p1((double)nf) / 32.0f;
-    f.x[1] = flog2p1((double)mf) / 32.0f;
-    f.x[2] = flog2p1((double)mu) / 32.0f;
-    f.x[3] = flog2p1((double)nf_prev) / 32.0f;
-    f.x[4] = (float)step / 16.0f;
-    f.x[5] = flog2p1((double)V) / 32.0f;
-    f.x[6] = flog2p1((double)E / (V > 0 ? V : 1)) / 8.0f;
+    const double v = V > 0 ? (double)V : 1.0, e = E > 0 ? (double)E : 1.0;
+    f.x[0] = (float)(log2(((double)mf + 1.0) / ((double)mu + 1.0)) / 8.0);
+    f.x[1] = (float)(log2(((double)nf + 1.0) / v) / 8.0);
+    f.x[2] = (float)(log2(((double)nf + 1.0) / ((double)nf_prev + 1.0)) / 8.0);
+    f.x[3] = flog2p1((double)step) / 8.0f;
+    f.x[4] = flog2p1(e / v) / 8.0f;
+    f.x[5] = (float)(log2(((double)mu + 1.0) / e) / 8.0);
+    f.x[6] = (float)(log2(((double)mf + 1.0) / e) / 8.0);
     f.x[7] = nf >= nf_prev ? 1.0f : 0.0f;
-    f.x[8] = (flog2p1((double)mf) - flog2p1((double)mu)) / 8.0f;
-    f.x[9] = (float)prev_dir;
+    f.x[8] = (float)prev_dir;
+    f.x[9] = (float)plain_dir;
     return f;
 }
 
-// SSSP bucket features: relaxation rounds so far, far-pile size, distance of
-// the nearest far entry relative to the current bound, delta, graph size and
-// mean degree.
+// SSSP bucket features, scale-free as well: relaxation rounds and buckets so
+// far, the far pile's share of the vertices, the gap from the current bound
+// to the nearest far entry and the bound itself in units of delta and of the
+// mean edge weight, mean degree, and the mean edge weight in units of delta
+// (how many buckets one edge spans).
 __host__ __device__ inline Feat sssp_features(int steps, unsigned long long far_len, float min_far, float thr,
-                                              float delta, int V, long long E, int buckets)
+                                              float delta, int V, long long E, int buckets, float mean_w)
 {
     Feat f;
-    f.x[0] = (float)steps / 64.0f;
-    f.x[1] = flog2p1((double)far_len) / 32.0f;
-    f.x[2] = (min_far - thr) / (delta > 0 ? delta : 1.0f) / 8.0f;
-    f.x[3] = thr / (delta > 0 ? delta : 1.0f) / 64.0f;
-    f.x[4] = flog2p1((double)V) / 32.0f;
-    f.x[5] = flog2p1((double)E / (V > 0 ? V : 1)) / 8.0f;
-    f.x[6] = (float)buckets / 64.0f;
-    f.x[7] = flog2p1((double)far_len) / (flog2p1((double)V) + 1.0f);
-    f.x[8] = delta;
+    const double d = delta > 0 ? (double)delta : 1.0;
+    const double mw = mean_w > 0 ? (double)mean_w : d;
+    const double v = V > 0 ? (double)V : 1.0;
+    const double gap = (double)min_far - (double)thr;
+    f.x[0] = flog2p1((double)steps) / 16.0f;
+    f.x[1] = (float)(log2(((double)far_len + 1.0) / v) / 8.0);
+    f.x[2] = fslog2p1(gap / d) / 16.0f;
+    f.x[3] = flog2p1((double)thr / d) / 16.0f;
+    f.x[4] = flog2p1((double)E / v) / 8.0f;
+    f.x[5] = flog2p1((double)buckets) / 16.0f;
+    f.x[6] = fslog2p1(mw / d) / 8.0f;
+    f.x[7] = fslog2p1(gap / mw) / 8.0f;
+    f.x[8] = flog2p1((double)thr / mw) / 16.0f;
     f.x[9] = 1.0f;
     return f;
 }
@@ -73,30 +87,42 @@ __host__ __device__ inline Feat sssp_features(int steps, unsigned long long far_
 __host__ __device__ inline float sssp_width_scale(int option) { return (float)(1 << (2 * option)); }
 
 #ifdef __CUDACC__
-// Warp-cooperative forward pass: lane j owns hidden unit j.  All 32 lanes
-// must call; every lane returns the argmax (lowest index on ties).  The
-// summation order is fixed, so every CTA computes the same decision.
-__device__ inline int mlp_argmax_warp(const float *__restrict__ p, const Feat &f, int O)
+// Warp-cooperative forward pass over parameters held in shared memory: lane j
+// owns hidden unit j; the output layer reduces all O logits in one butterfly
+// (O independent shuffle chains).  All 32 lanes must call; lane 0's argmax
+// (lowest index on ties) is returned in every lane.  The summation order is
+// fixed, so every CTA computes the same decision.
+template <int O>
+__device__ inline int mlp_argmax_warp(const float *p, const Feat &f)
 {
     const int j = threadIdx.x & 31;
     const float *W1 = p, *b1 = W1 + kHidden * kFeat, *W2 = b1 + kHidden, *b2 = W2 + kHidden * kHidden;
     const float *W3 = b2 + kHidden, *b3 = W3 + O * kHidden;
-    float a = __ldg(&b1[j]);
+    float a = b1[j];
 #pragma unroll
-    for (int i = 0; i < kFeat; i++) a = fmaf(__ldg(&W1[j * kFeat + i]), f.x[i], a);
+    for (int i = 0; i < kFeat; i++) a = fmaf(W1[j * kFeat + i], f.x[i], a);
     const float h1 = tanhf(a);
-    a = __ldg(&b2[j]);
-#pragma unroll 8
-    for (int i = 0; i < kHidden; i++) a = fmaf(__ldg(&W2[j * kHidden + i]), __shfl_sync(0xffffffffu, h1, i), a);
+    a = b2[j];
+#pragma unroll
+    for (int i = 0; i < kHidden; i++) a = fmaf(W2[j * kHidden + i], __shfl_sync(0xffffffffu, h1, i), a);
     const float h2 = tanhf(a);
+    float t[O];
+#pragma unroll
+    for (int o = 0; o < O; o++) t[o] = W3[o * kHidden + j] * h2;
+#pragma unroll
+    for (int s = 16; s; s >>= 1) {
+#pragma unroll
+        for (int o = 0; o < O; o++) t[o] += __shfl_xor_sync(0xffffffffu, t[o], s);
+    }
     int best = 0;
     float bestv = -INFINITY;
-    for (int o = 0; o < O; o++) {
-        float t = __ldg(&W3[o * kHidden + j]) * h2;
 #pragma unroll
-        for (int s = 16; s; s >>= 1) t += __shfl_xor_sync(0xffffffffu, t, s);
-        t += __ldg(&b3[o]);
-        if (t > bestv) { bestv = t; best = o; }
+    for (int o = 0; o < O; o++) {
+        const float v = t[o] + b3[o];
+        if (v > bestv) {
+            bestv = v;
+            best = o;
+        }
     }
     // the butterfly sums may round differently per lane: lane 0 decides
     return __shfl_sync(0xffffffffu, best, 0);

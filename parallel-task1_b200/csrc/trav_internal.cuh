@@ -88,6 +88,7 @@ struct DevGraph {
     int32_t V = 0;
     int64_t E = 0;
     int32_t max_out_degree = 0;
+    float mean_w = 0.0f;          // mean edge weight (a schedule feature)
     int32_t *out_off = nullptr;   // V+1
     int32_t *out_adj = nullptr;   // E
     float *out_w = nullptr;       // E
@@ -156,6 +157,7 @@ struct TravArgs {
     int32_t force_dir;
     // SSSP options
     float delta;           // +inf = Bellman-Ford
+    float mean_w;          // mean edge weight of the graph
     // output (original ids); nullptr = leave results in `value`
     void *out;
     int32_t out_kind;      // 0 = int32 levels, 1 = float distances, 2 = uint8 reached flags
@@ -184,6 +186,7 @@ struct BatchQuery {
     int32_t kind;           // 0 = BFS, 1 = SSSP
     int32_t source;         // new id
     float delta;            // SSSP bucket width (+inf = Bellman-Ford)
+    float mean_w;           // mean edge weight
 };
 
 // Scratch of one team of a batch launch, sized for the batch's largest graph.

@@ -863,12 +863,21 @@ __device__ __forceinline__ void init_counters(CtaCounters &cc)
 // Shared memory of one query's CTA (the bodies below run inside the
 // single-query kernels and inside the batch kernel).
 struct QueryShared {
+    float mlp[kMlpMaxParams];  // the schedule network, copied in when the query has one
     WarpStage wst[kWarps];
     CtaCounters cc;
     SlotView view;
     int dir;
     float bound;
 };
+
+// Copy the query's schedule network into shared memory (read there by warp 0
+// at every decision); the first grid barrier orders it before any use.
+__device__ __forceinline__ void load_mlp(const TravArgs &a, QueryShared &sh, int count)
+{
+    if (!a.mlp) return;
+    for (int i = threadIdx.x; i < count; i += kBlock) sh.mlp[i] = __ldg(&a.mlp[i]);
+}
 
 // One query on the CTAs [a.cta0, a.cta0 + a.ctas), starting at phase ph0 of the
 // counter-slot ring.  Returns the next phase index, or -1 when the query failed
@@ -888,6 +897,7 @@ __device__ __forceinline__ int bfs_query(const TravArgs &a, QueryShared &sh, int
     const int s = a.source;
     int ph = ph0;
 
+    load_mlp(a, sh, mlp_param_count(kBfsOut));
     init_counters(cc);
     for (int v = gtid; v < a.V; v += nth) reinterpret_cast<int *>(a.value)[v] = v == s ? 0 : -1;
     for (int w = gtid; w < a.W; w += nth) a.visited[w] = w == (s >> 5) ? 1u << (s & 31) : 0u;
@@ -908,12 +918,16 @@ __device__ __forceinline__ int bfs_query(const TravArgs &a, QueryShared &sh, int
         }
         // direction for this step (same inputs in every CTA -> same answer)
         if (threadIdx.x < 32) {
-            const Feat f = bfs_features(L, nf, mf, mu, nf_prev, a.V, a.E, prev_dir);
-            int d = dir;
+            int plain = dir;  // Beamer's switch
+            if (dir == 0) {
+                if ((double)mf > (double)mu / a.alpha) plain = 1;
+            } else if (!(nf >= nf_prev || (double)nf > (double)a.V / a.beta)) {
+                plain = 0;
+            }
+            const Feat f = bfs_features(L, nf, mf, mu, nf_prev, a.V, a.E, prev_dir, plain);
+            int d = plain;
             if (a.force_dir >= 0) d = (L == 0) ? 0 : a.force_dir;
-            else if (a.mlp) d = mlp_argmax_warp(a.mlp, f, kBfsOut);
-            else if (dir == 0) { if ((double)mf > (double)mu / a.alpha) d = 1; }
-            else if (!(nf >= nf_prev || (double)nf > (double)a.V / a.beta)) d = 0;
+            else if (a.mlp) d = mlp_argmax_warp<kBfsOut>(sh.mlp, f);
             const int forced = planned(a, L);
             if (forced >= 0) d = forced;
             log_decision(ctl, lg, f, d, 0.0f, 0.0f);
@@ -1085,6 +1099,7 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, in
     const int lpart = a.nlight ? kPartLight : kPartWhole;
     const unsigned big_len = (unsigned)a.small_deg + 1u;  // any length that classifies as a long row
     int ph = ph0;
+    load_mlp(a, sh, mlp_param_count(kSsspOut));
     init_counters(cc);
     unsigned nq, nch, nbig;                 // current frontier (light parts)
     unsigned hq = 0, hch = 0, hbig = 0;     // heavy list of the current round
@@ -1096,7 +1111,10 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, in
     unsigned h_start = 1, f_start = 1;      // rounds the heavy list / far pile began in
     if (a.source >= 0) {
         const int s = a.source;
-        for (int v = gtid; v < a.V; v += nth) a.dist[v] = pack_dist(v == s ? 0.0f : FLT_MAX, row_class(a, v));
+        for (int v = gtid; v < a.V; v += nth) {
+            const unsigned cls = row_class(a, v);
+            a.dist[v] = pack_dist(v == s ? 0.0f : FLT_MAX, cls);
+        }
         const int2 lp = row_part(a, s, lpart);
         seed_part(a, s, lp.x, lp.y, a.q0, a.chunks0, nq, nch);
         nbig = nch ? 1u : 0u;
@@ -1213,9 +1231,9 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, in
         } else if (far_len > 0) {
             // open the next bucket (skipping empty ones): bound = max(old, min far) + width
             if (threadIdx.x < 32) {
-                const Feat f = sssp_features(steps, far_len, __int_as_float(min_far), thr, a.delta, a.V, a.E, buckets);
+                const Feat f = sssp_features(steps, far_len, __int_as_float(min_far), thr, a.delta, a.V, a.E, buckets, a.mean_w);
                 int o = 0;
-                if (a.mlp) o = mlp_argmax_warp(a.mlp, f, kSsspOut);
+                if (a.mlp) o = mlp_argmax_warp<kSsspOut>(sh.mlp, f);
                 const int forced = planned(a, buckets - 1);
                 if (forced >= 0) o = forced;
                 const float width = a.delta * sssp_width_scale(o);
@@ -1370,6 +1388,7 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) batch_persistent
             a.max_steps = (int32_t)min((long long)4 * q.V + 4096, (long long)(kMaxRounds - 2 - ph));
             a.force_dir = -1;
             a.delta = q.delta;
+            a.mean_w = q.mean_w;
             a.out_kind = 1;
             ph = sssp_query(a, sh, ph);
         }
@@ -1479,6 +1498,36 @@ int device_timeout_err(const Ctl &h, const char *what)
     return TRAV_OK;
 }
 
+// Record a timing event; inside a stream capture it becomes an event-record
+// node of the graph (an external record), so every replay records it.
+int record_event(cudaEvent_t ev, cudaStream_t st)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    TRY_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs == cudaStreamCaptureStatusActive) TRY_CUDA(cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal));
+    else TRY_CUDA(cudaEventRecord(ev, st));
+    return TRAV_OK;
+}
+
+// A cooperative launch (every CTA co-resident, which the grid barriers need),
+// issued through the attribute form so that it can also be captured into a
+// CUDA graph.
+int launch_cooperative(const void *fn, int grid, void **params, cudaStream_t st)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kBlock);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    TRY_CUDA(cudaLaunchKernelExC(&cfg, fn, params));
+    return TRAV_OK;
+}
+
 // Enqueue one persistent launch: clear its control block, launch
 // cooperatively (all CTAs co-resident, which the grid barrier needs).
 int enqueue_persistent(int kind, TravArgs &args, int ctas, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1)
@@ -1489,11 +1538,10 @@ int enqueue_persistent(int kind, TravArgs &args, int ctas, cudaStream_t st, cuda
     args.cta0 = 0;
     args.ctas = grid;
     TRY_CUDA(cudaMemsetAsync(args.ctl, 0, offsetof(Ctl, dirs), st));
-    if (ev0) TRY_CUDA(cudaEventRecord(ev0, st));
+    if (ev0) TRY(record_event(ev0, st));
     void *params[] = {&args};
-    TRY_CUDA(cudaLaunchCooperativeKernel(kind == 0 ? (void *)bfs_persistent : (void *)sssp_persistent, dim3(grid),
-                                         dim3(kBlock), params, 0, st));
-    if (ev1) TRY_CUDA(cudaEventRecord(ev1, st));
+    TRY(launch_cooperative(kind == 0 ? (const void *)bfs_persistent : (const void *)sssp_persistent, grid, params, st));
+    if (ev1) TRY(record_event(ev1, st));
     return TRAV_OK;
 }
 
@@ -1550,8 +1598,7 @@ int launch_batch(BatchArgs b, int teams, cudaStream_t st, cudaEvent_t ev0, cudaE
     TRY_CUDA(cudaMemsetAsync(b.next, 0, sizeof(unsigned), st));
     if (ev0) TRY_CUDA(cudaEventRecord(ev0, st));
     void *params[] = {&b};
-    TRY_CUDA(cudaLaunchCooperativeKernel((void *)batch_persistent, dim3(teams * b.team_ctas), dim3(kBlock), params, 0,
-                                         st));
+    TRY(launch_cooperative((const void *)batch_persistent, teams * b.team_ctas, params, st));
     if (ev1) TRY_CUDA(cudaEventRecord(ev1, st));
     return TRAV_OK;
 }
@@ -1575,6 +1622,7 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
     ws->V = g.V;
     ws->chunk_cap = V + g.E / kMinItem + 1;
     TRY_CUDA(cudaMalloc(&ws->value, sizeof(unsigned long long) * V));
+
     TRY_CUDA(cudaMalloc(&ws->visited, sizeof(unsigned) * W));
     TRY_CUDA(cudaMalloc(&ws->front[0], sizeof(unsigned) * W));
     TRY_CUDA(cudaMalloc(&ws->front[1], sizeof(unsigned) * W));
@@ -1648,6 +1696,7 @@ static TravArgs make_args(const DevGraph &g, Workspace *ws)
     a.chunks0 = ws->chunks[0];
     a.chunks1 = ws->chunks[1];
     a.timeout_ns = 10ull * 1000000000ull;
+    a.mean_w = g.mean_w;
     a.cta0 = 0;
     a.ctas = 0;  // set at launch
     a.small_deg = ws->small_deg;

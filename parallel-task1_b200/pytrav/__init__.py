@@ -38,6 +38,7 @@ TRAV_ERR_NO_DEVICE = -6
 TRAV_ERR_IO = -7
 MEM_HOST, MEM_DEVICE = 0, 1
 SCHEDULE_PLAIN, SCHEDULE_LEARNED = 0, 1
+MLP_OUTPUTS = (2, 6)  # schedule network outputs: BFS direction, SSSP bucket width delta * 4^k
 FLT_MAX = np.float32(np.finfo(np.float32).max)
 
 # Every symbol include/trav.h declares (checked by the CPU test suite).
@@ -48,7 +49,7 @@ EXPORTS = [
     "trav_mlp_param_count", "trav_last_error", "trav_version", "trav_last_batch_ms", "trav_graph_set_stream",
     "trav_bfs_csr_noalloc", "trav_last_phase_log", "trav_mlp_loss_grad", "trav_mlp_train", "trav_set_plan",
     "trav_last_decisions", "trav_set_grid", "trav_batch_create", "trav_batch_free", "trav_batch_run",
-    "trav_batch_autotune", "trav_batch_set_shape", "trav_batch_get_shape",
+    "trav_batch_autotune", "trav_batch_set_shape", "trav_batch_get_shape", "trav_graph_set_capture",
 ]
 
 
@@ -112,6 +113,7 @@ def lib():
         L.trav_el_file_write.argtypes = [C.c_char_p, i32, i32, i64, vp, vp, vp]
         L.trav_mlp_set.argtypes = [vp, i32, vp, i32]
         L.trav_set_grid.argtypes = [vp, i32, i32, C.POINTER(i32)]
+        L.trav_graph_set_capture.argtypes = [vp, i32]
         L.trav_batch_create.argtypes = [C.POINTER(vp), i32, C.POINTER(vp)]
         L.trav_batch_free.argtypes = [vp]
         L.trav_batch_free.restype = None
@@ -277,6 +279,10 @@ class Graph:
         k = min(n.value, cap)
         return kind[:k].copy(), size[:k].copy(), end[:k].copy(), edges[:k].copy()
 
+    def set_capture(self, on: bool = True):
+        """Record calls with device outputs into CUDA graphs and replay them while their arguments repeat."""
+        _check(lib().trav_graph_set_capture(self._h, 1 if on else 0))
+
     def set_grid(self, kind: int, ctas: int = 0) -> int:
         """CTAs of later `kind` launches (0 = as many as fit); returns that maximum."""
         most = C.c_int32(0)
@@ -359,7 +365,7 @@ def mlp_train(kind: int, params, x, labels, epochs: int = 500, lr: float = 1e-2)
 def mlp_init(kind: int, seed: int = 0):
     """Glorot-uniform weights, zero biases, in the packed layout."""
     rng = np.random.default_rng(seed)
-    F, H, O = MLP_FEATURES, 32, (2 if kind == 0 else 4)
+    F, H, O = MLP_FEATURES, 32, MLP_OUTPUTS[kind]
     parts = []
     for fan_in, fan_out in ((F, H), (H, H), (H, O)):
         lim = np.sqrt(6.0 / (fan_in + fan_out))

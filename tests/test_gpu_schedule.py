@@ -46,7 +46,7 @@ def test_forced_sssp_widths_keep_distances(graph):
     g, src, _, want_d = graph
     rng = np.random.default_rng(1)
     for _ in range(12):
-        plan = rng.integers(0, 4, 64).astype(np.uint8)
+        plan = rng.integers(0, 6, 64).astype(np.uint8)
         g.set_plan(1, plan)
         got = g.sssp([src], delta=0.05)[0]
         assert np.array_equal(got.view(np.uint32), want_d)
@@ -91,3 +91,31 @@ def test_grid_size_keeps_results(graph):
         g.set_grid(0, most + 1)
     g.set_grid(0, 0)
     g.set_grid(1, 0)
+
+
+def test_cuda_graph_capture_replays_same_results(graph):
+    import torch
+
+    g, src, want_lv, want_d = graph
+    srcs = [src, (src + 17) % g.V, (src + 101) % g.V]
+    ref_lv = g.bfs(srcs)
+    ref_d = g.sssp(srcs, delta=0.05)
+    lv = torch.empty((len(srcs), g.V), dtype=torch.int32, device="cuda")
+    di = torch.empty((len(srcs), g.V), dtype=torch.float32, device="cuda")
+    g.set_capture(True)
+    try:
+        for delta in (0.05, 0.05, 0.2, 0.05):  # record, replay, record anew, record anew
+            lv.fill_(7)
+            di.fill_(7)
+            g.bfs(srcs, out=lv)
+            g.sssp(srcs, out=di, delta=delta)
+            assert np.array_equal(lv.cpu().numpy(), ref_lv)
+            if delta == 0.05:
+                assert np.array_equal(di.cpu().numpy().view(np.uint32), ref_d.view(np.uint32))
+            assert len(g.last_batch_ms()) == len(srcs)
+        # an uncaptured call with another delta after a replay still counts its own light prefixes
+        g.set_capture(False)
+        assert np.array_equal(g.sssp([src], delta=0.3)[0].view(np.uint32), want_d)
+        assert np.array_equal(g.sssp(srcs, delta=0.05).view(np.uint32), ref_d.view(np.uint32))
+    finally:
+        g.set_capture(False)

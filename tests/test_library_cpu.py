@@ -41,7 +41,7 @@ def test_reference_cxx_wrappers_exported():
 def test_version_and_param_counts():
     assert b"sm_100a" in T.lib().trav_version()
     assert T.mlp_param_count(0) == 32 * 10 + 32 + 32 * 32 + 32 + 2 * 32 + 2
-    assert T.mlp_param_count(1) == 32 * 10 + 32 + 32 * 32 + 32 + 4 * 32 + 4
+    assert T.mlp_param_count(1) == 32 * 10 + 32 + 32 * 32 + 32 + 6 * 32 + 6
     assert T.mlp_param_count(7) == -1
 
 

@@ -11,7 +11,7 @@ F, H = 10, 32
 
 def _problem(kind, n, seed):
     rng = np.random.default_rng(seed)
-    Oo = 2 if kind == 0 else 4
+    Oo = T.MLP_OUTPUTS[kind]
     p = T.mlp_init(kind, seed).astype(np.float64) if False else None
     x = rng.normal(size=(n, F))
     y = rng.integers(0, Oo, n).astype(np.int32)
@@ -20,7 +20,7 @@ def _problem(kind, n, seed):
 
 def _init64(kind, seed):
     rng = np.random.default_rng(seed)
-    Oo = 2 if kind == 0 else 4
+    Oo = T.MLP_OUTPUTS[kind]
     sizes = [H * F, H, H * H, H, Oo * H, Oo]
     return np.concatenate([rng.normal(scale=0.3, size=s) for s in sizes])
 
@@ -41,7 +41,7 @@ def test_oracle_gradient_matches_finite_differences(kind):
 
 
 def test_param_layout_counts_match_library():
-    for kind, Oo in ((0, 2), (1, 4)):
+    for kind, Oo in ((0, 2), (1, 6)):
         assert T.mlp_param_count(kind) == H * F + H + H * H + H + Oo * H + Oo
         assert len(T.mlp_init(kind)) == T.mlp_param_count(kind)
 
