@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched many-graph measurement")
+    ap.add_argument("--batched-only", action="store_true", help="run only the batched many-graph measurement")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="target seconds of CPU baseline work")
     return ap.parse_args()
 
@@ -261,6 +262,10 @@ def run_ours(a):
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
+    if a.batched_only:
+        if rank == 0:
+            print(json.dumps({"batched": batched_workload(a.seed)}), flush=True)
+        return
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     dev = torch.device("cuda", local)

@@ -28,10 +28,15 @@ struct Feat {
     float x[kFeat];
 };
 
-__host__ __device__ inline float flog2p1(double v) { return (float)log2(1.0 + (v > 0 ? v : 0)); }
+// Feature arithmetic is single precision (log2f): the features only steer a
+// choice, and every CTA evaluates them identically.
+__host__ __device__ inline float flog2p1(double v) { return log2f(1.0f + (float)(v > 0 ? v : 0)); }
 
 // sign(v) * log2(1 + |v|): bounded growth for quantities of any scale
 __host__ __device__ inline float fslog2p1(double v) { return v < 0 ? -flog2p1(-v) : flog2p1(v); }
+
+// log2(a / b) for counts (a, b >= 1)
+__host__ __device__ inline float flog2ratio(double a, double b) { return log2f((float)a) - log2f((float)b); }
 
 // BFS step features, all scale-free so that graphs larger than the training
 // graphs stay in range: the two ratios Beamer's switch tests (frontier
@@ -45,24 +50,25 @@ __host__ __device__ inline Feat bfs_features(int step, unsigned long long nf, un
 {
     Feat f;
     const double v = V > 0 ? (double)V : 1.0, e = E > 0 ? (double)E : 1.0;
-    f.x[0] = (float)(log2(((double)mf + 1.0) / ((double)mu + 1.0)) / 8.0);
-    f.x[1] = (float)(log2(((double)nf + 1.0) / v) / 8.0);
-    f.x[2] = (float)(log2(((double)nf + 1.0) / ((double)nf_prev + 1.0)) / 8.0);
+    f.x[0] = flog2ratio((double)mf + 1.0, (double)mu + 1.0) / 8.0f;
+    f.x[1] = flog2ratio((double)nf + 1.0, v) / 8.0f;
+    f.x[2] = flog2ratio((double)nf + 1.0, (double)nf_prev + 1.0) / 8.0f;
     f.x[3] = flog2p1((double)step) / 8.0f;
     f.x[4] = flog2p1(e / v) / 8.0f;
-    f.x[5] = (float)(log2(((double)mu + 1.0) / e) / 8.0);
-    f.x[6] = (float)(log2(((double)mf + 1.0) / e) / 8.0);
+    f.x[5] = flog2ratio((double)mu + 1.0, e) / 8.0f;
+    f.x[6] = flog2ratio((double)mf + 1.0, e) / 8.0f;
     f.x[7] = nf >= nf_prev ? 1.0f : 0.0f;
     f.x[8] = (float)prev_dir;
     f.x[9] = (float)plain_dir;
     return f;
 }
 
-// SSSP bucket features, scale-free as well: relaxation rounds and buckets so
-// far, the far pile's share of the vertices, the gap from the current bound
-// to the nearest far entry and the bound itself in units of delta and of the
-// mean edge weight, mean degree, and the mean edge weight in units of delta
-// (how many buckets one edge spans).
+// SSSP bucket features: relaxation rounds and buckets so far, the far pile's
+// share of the vertices, the gap from the current bound to the nearest far
+// entry and the bound itself in units of delta and of the mean edge weight,
+// mean degree, the mean edge weight in units of delta (how many buckets one
+// edge spans), and the graph's size: whether wide buckets pay depends on it,
+// since they trade fewer rounds (latency) for more re-relaxation (work).
 __host__ __device__ inline Feat sssp_features(int steps, unsigned long long far_len, float min_far, float thr,
                                               float delta, int V, long long E, int buckets, float mean_w)
 {
@@ -72,7 +78,7 @@ __host__ __device__ inline Feat sssp_features(int steps, unsigned long long far_
     const double v = V > 0 ? (double)V : 1.0;
     const double gap = (double)min_far - (double)thr;
     f.x[0] = flog2p1((double)steps) / 16.0f;
-    f.x[1] = (float)(log2(((double)far_len + 1.0) / v) / 8.0);
+    f.x[1] = flog2ratio((double)far_len + 1.0, v) / 8.0f;
     f.x[2] = fslog2p1(gap / d) / 16.0f;
     f.x[3] = flog2p1((double)thr / d) / 16.0f;
     f.x[4] = flog2p1((double)E / v) / 8.0f;
@@ -80,7 +86,7 @@ __host__ __device__ inline Feat sssp_features(int steps, unsigned long long far_
     f.x[6] = fslog2p1(mw / d) / 8.0f;
     f.x[7] = fslog2p1(gap / mw) / 8.0f;
     f.x[8] = flog2p1((double)thr / mw) / 16.0f;
-    f.x[9] = 1.0f;
+    f.x[9] = flog2p1((double)E) / 32.0f;
     return f;
 }
 
