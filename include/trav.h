@@ -271,6 +271,29 @@ int trav_last_decisions(trav_graph *g, float *x, uint8_t *choice, int32_t *phase
 const char *trav_last_error(void);
 const char *trav_version(void);
 
+/* ------------------------------------------------------ graph optimisation
+ * The optimisation pass of GraphOptimizationAPI on an edge list, in place
+ * (replaces remove_loops_and_multiple_arcs and reorder_edges_for_cache,
+ * include/test/optimization/graph_optimization_API.hpp:60-166): edges are
+ * sorted by (src, dst, weight), self-loops and repeated arcs are dropped (the
+ * lightest arc of each (src, dst) pair stays), and when segment > 0 the edges
+ * are grouped by (src / segment, dst / segment) -- the reference's segment is
+ * its L2 size / elem_size vertices -- keeping the (src, dst, weight) order
+ * inside a group.  Weights of -0.0 become +0.0.  *edges_out receives the new
+ * count; the arrays keep their capacity.  mem says where the arrays live
+ * (TRAV_MEM_HOST arrays are copied to the device and back). */
+int trav_el_optimize(int32_t *src, int32_t *dst, float *w, int32_t vertices, int64_t edges, int32_t segment,
+                     int32_t mem, int64_t *edges_out);
+
+/* Memory transactions of an edge-per-thread sweep over an edge list
+ * (replaces check_gpu_memory_transactions_count,
+ * graph_optimization_API.hpp:229-266): for each warp of 32 consecutive edges,
+ * the distinct 128-byte segments among src * elem_size plus those among
+ * dst * elem_size.  As in the reference, the warp holding the last edge is
+ * not counted. */
+int trav_el_gpu_transactions(const int32_t *src, const int32_t *dst, int32_t vertices, int64_t edges,
+                             int32_t elem_size, int32_t mem, int64_t *count);
+
 /* ----------------------------------------------------------------- batches
  * Many BFS / SSSP queries over several graphs in one persistent launch.  The
  * launch is cut into teams of CTAs; each team runs one query at a time and

@@ -57,6 +57,10 @@ def lib():
         L.orc_bfs_bytes.argtypes = [C.c_int32, _i64p, _i64p, _i32p, _i32p, _u8p, C.c_int]
         L.orc_bfs_bytes.restype = C.c_int64
         L.orc_mlp_loss_grad.argtypes = [C.c_int, C.c_int, C.c_int, _f64p, C.c_int, _f64p, _i32p, C.c_void_p]
+        L.orc_el_optimize.argtypes = [C.c_int64, _i32p, _i32p, _f32p, C.c_int32, _i32p, _i32p, _f32p]
+        L.orc_el_optimize.restype = C.c_int64
+        L.orc_gpu_transactions.argtypes = [C.c_int64, _i32p, _i32p, C.c_int32]
+        L.orc_gpu_transactions.restype = C.c_int64
         L.orc_mlp_loss_grad.restype = C.c_double
         _orc = L
     return _orc
@@ -95,6 +99,10 @@ def ref():
         L.ref_save_edges_list.argtypes = [vp, C.c_char_p]
         L.ref_save_adjacency_list.argtypes = [vp, C.c_char_p]
         L.ref_load_edges_list.argtypes = [C.c_char_p]
+        L.ref_optimize_for_cpu.argtypes = [vp, C.c_int]
+        L.ref_optimize_for_cpu.restype = C.c_longlong
+        L.ref_gpu_transactions.argtypes = [vp, C.c_int]
+        L.ref_gpu_transactions.restype = C.c_longlong
         L.ref_load_edges_list.restype = vp
         L.ref_wtime.restype = C.c_double
         _ref = L
@@ -177,6 +185,21 @@ def bfs_bytes(V, layout, levels_new, dirs):
                                    _c(levels_new, np.int32), dirs, len(dirs)))
 
 
+def el_optimize(src, dst, w, segment=0):
+    """Graph optimisation pass: (src, dst, w) sorted by (src, dst, w) without loops and repeated arcs, then
+    grouped by (src // segment, dst // segment) when segment > 0."""
+    E = len(src)
+    s, d, ww = _c(src, np.int32), _c(dst, np.int32), _c(w, np.float32)
+    os_, od, ow = np.empty(max(E, 1), np.int32), np.empty(max(E, 1), np.int32), np.empty(max(E, 1), np.float32)
+    n = lib().orc_el_optimize(E, s, d, ww, segment, os_, od, ow)
+    return os_[:n].copy(), od[:n].copy(), ow[:n].copy()
+
+
+def gpu_transactions(src, dst, elem_size=4):
+    """Distinct 128-byte segments per warp of 32 consecutive edges, summed (the last warp excluded)."""
+    return int(lib().orc_gpu_transactions(len(src), _c(src, np.int32), _c(dst, np.int32), elem_size))
+
+
 def mlp_loss_grad(F, H, O, params, x, labels, want_grad=True):
     params = _c(params, np.float64)
     x = _c(x, np.float64)
@@ -228,6 +251,19 @@ class RefGraph:
         r = np.empty(self.V, np.uint8)
         assert ref().ref_cpu_sequential_bfs(self.h, source, r) == 0
         return r
+
+    def optimize_for_cpu(self, elem_size=4):
+        """The reference's optimize_graph_for_CPU on this edge-list graph (in place); returns the new edge count."""
+        self.E = int(ref().ref_optimize_for_cpu(self.h, elem_size))
+        return self.E
+
+    def gpu_transactions(self, elem_size=4):
+        return int(ref().ref_gpu_transactions(self.h, elem_size))
+
+    def export_el(self):
+        s, d, w = np.empty(max(self.E, 1), np.int32), np.empty(max(self.E, 1), np.int32), np.empty(max(self.E, 1), np.float32)
+        ref().ref_graph_export_el(self.h, s, d, w)
+        return s[:self.E], d[:self.E], w[:self.E]
 
     def parallel_bfs(self, source, threads=0):
         r = np.empty(self.V, np.uint8)

@@ -14,6 +14,8 @@
 //   GraphGenerationAPI::R_MAT_parallel            include/test/generation/graph_generation_API.hpp:403-484
 //   GraphStorageAPI::{save,load}_*_bin_file       include/storage/graph_storage_API.hpp:3-160
 //   Graph::convert_to_compressed_adjacency_list   include/graph_data_structures/graph.hpp:316-361
+//   GraphOptimizationAPI::optimize_graph_for_CPU  include/test/optimization/graph_optimization_API.hpp:173-224
+//   GraphOptimizationAPI::check_gpu_memory_transactions_count                             :229-266
 #include <cstdint>
 #include <cstring>
 #include <cfloat>
@@ -28,6 +30,7 @@
 #include "include/storage/graph_storage_API.h"
 #include "algorithm/sssp/sssp.h"
 #include "algorithm/bfs/bfs.h"
+#include "include/test/optimization/graph_optimization_API.h"
 
 typedef Graph<int, float> RefGraph;
 
@@ -171,5 +174,20 @@ int ref_graph_export_el(void *h, int *src, int *dst, float *w)
 }
 
 double ref_wtime(void) { return omp_get_wtime(); }
+
+// The reference's CPU optimisation pass on an edge-list graph, in place
+// (loops and repeated arcs removed, edges grouped by CPU_L2_CACHE_SIZE /
+// elem_size vertex segments).  Returns the new edge count.
+long long ref_optimize_for_cpu(void *h, int elem_size)
+{
+    RefGraph *g = (RefGraph *)h;
+    GraphOptimizationAPI<int, float>::optimize_graph_for_CPU(*g, elem_size);
+    return g->get_edges_count();
+}
+
+long long ref_gpu_transactions(void *h, int elem_size)
+{
+    return GraphOptimizationAPI<int, float>::check_gpu_memory_transactions_count(*(RefGraph *)h, elem_size);
+}
 
 }  // extern "C"

@@ -401,3 +401,92 @@ double orc_mlp_loss_grad(int F, int H, int O, const double *params, int n, const
     free(h1); free(h2); free(y); free(dy); free(d2); free(d1);
     return loss / n;
 }
+
+/* ---------------------------------------------------------------- graph optimisation
+ * GraphOptimizationAPI (include/test/optimization/graph_optimization_API.hpp):
+ *   reorder_edges_in_adjacency_list_format :14-55  sort edges by (src, dst, weight)
+ *   remove_loops_and_multiple_arcs          :60-117 drop loops; drop an edge whose (src, dst) equals the
+ *                                                   previous sorted edge's (so the lightest arc is kept)
+ *   reorder_edges_for_cache                 :122-166 sort by (src / seg, dst / seg); std::sort leaves the
+ *                                                   order inside a segment pair unspecified -- here it is the
+ *                                                   (src, dst, weight) order (a stable sort)
+ * Weights compare as floats; -0.0 is read as +0.0 first so that equal weights have equal bits. */
+typedef struct {
+    int32_t s, d;
+    float w;
+    int64_t pos;
+} opt_edge;
+
+static int cmp_sdw(const void *pa, const void *pb)
+{
+    const opt_edge *a = (const opt_edge *)pa, *b = (const opt_edge *)pb;
+    if (a->s != b->s) return a->s < b->s ? -1 : 1;
+    if (a->d != b->d) return a->d < b->d ? -1 : 1;
+    if (a->w != b->w) return a->w < b->w ? -1 : 1;
+    return a->pos < b->pos ? -1 : (a->pos > b->pos);
+}
+
+static int32_t g_seg;
+static int cmp_segments(const void *pa, const void *pb)
+{
+    const opt_edge *a = (const opt_edge *)pa, *b = (const opt_edge *)pb;
+    const int32_t sa = a->s / g_seg, sb = b->s / g_seg, da = a->d / g_seg, db = b->d / g_seg;
+    if (sa != sb) return sa < sb ? -1 : 1;
+    if (da != db) return da < db ? -1 : 1;
+    return a->pos < b->pos ? -1 : (a->pos > b->pos);
+}
+
+int64_t orc_el_optimize(int64_t E, const int32_t *src, const int32_t *dst, const float *w, int32_t segment,
+                        int32_t *out_src, int32_t *out_dst, float *out_w)
+{
+    opt_edge *e = (opt_edge *)malloc(sizeof(opt_edge) * (size_t)(E > 0 ? E : 1));
+    for (int64_t i = 0; i < E; i++) {
+        e[i].s = src[i];
+        e[i].d = dst[i];
+        e[i].w = w[i] == 0.0f ? 0.0f : w[i];
+        e[i].pos = i;
+    }
+    qsort(e, (size_t)E, sizeof(opt_edge), cmp_sdw);
+    int64_t n = 0;
+    for (int64_t i = 0; i < E; i++) {
+        if (e[i].s == e[i].d) continue;
+        if (i > 0 && e[i].s == e[i - 1].s && e[i].d == e[i - 1].d) continue;
+        e[n] = e[i];
+        e[n].pos = n;
+        n++;
+    }
+    if (segment > 0) {
+        g_seg = segment;
+        qsort(e, (size_t)n, sizeof(opt_edge), cmp_segments);
+    }
+    for (int64_t i = 0; i < n; i++) {
+        out_src[i] = e[i].s;
+        out_dst[i] = e[i].d;
+        out_w[i] = e[i].w;
+    }
+    free(e);
+    return n;
+}
+
+/* check_gpu_memory_transactions_count (graph_optimization_API.hpp:229-266): for each warp of 32 consecutive
+ * edges, the distinct 128-byte segments of src * elem_size plus those of dst * elem_size.  The reference adds a
+ * warp's count when the next warp starts, so the warp holding the last edge is never added; kept. */
+int64_t orc_gpu_transactions(int64_t E, const int32_t *src, const int32_t *dst, int32_t elem_size)
+{
+    const int64_t counted = E > 0 ? (E - 1) / 32 : 0;  /* warps before the one holding the last edge */
+    int64_t total = 0;
+    for (int64_t k = 0; k < counted; k++) {
+        int64_t ss[32], ds[32];
+        int ns = 0, nd = 0;
+        for (int64_t i = 32 * k; i < 32 * k + 32; i++) {
+            const int64_t a = (int64_t)src[i] * elem_size / 128, b = (int64_t)dst[i] * elem_size / 128;
+            int j;
+            for (j = 0; j < ns && ss[j] != a; j++) {}
+            if (j == ns) ss[ns++] = a;
+            for (j = 0; j < nd && ds[j] != b; j++) {}
+            if (j == nd) ds[nd++] = b;
+        }
+        total += ns + nd;
+    }
+    return total;
+}

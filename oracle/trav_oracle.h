@@ -76,6 +76,15 @@ int64_t orc_bfs_bytes(int32_t V, const int64_t *out_off, const int64_t *in_off, 
 double orc_mlp_loss_grad(int F, int H, int O, const double *params, int n, const double *x,
                          const int32_t *label, double *grad);
 
+
+/* Graph optimisation pass (GraphOptimizationAPI): sort by (src, dst, w), drop loops and repeated arcs,
+ * then (segment > 0) group by (src / segment, dst / segment).  Returns the new edge count. */
+int64_t orc_el_optimize(int64_t E, const int32_t *src, const int32_t *dst, const float *w, int32_t segment,
+                        int32_t *out_src, int32_t *out_dst, float *out_w);
+
+/* check_gpu_memory_transactions_count: distinct 128-byte segments per warp of 32 edges (last warp excluded). */
+int64_t orc_gpu_transactions(int64_t E, const int32_t *src, const int32_t *dst, int32_t elem_size);
+
 #ifdef __cplusplus
 }
 #endif

@@ -453,6 +453,76 @@ int trav_graph_set_stream(trav_graph *g, void *stream)
     return TRAV_OK;
 }
 
+int trav_el_optimize(int32_t *src, int32_t *dst, float *w, int32_t vertices, int64_t edges, int32_t segment,
+                     int32_t mem, int64_t *edges_out)
+{
+    TRY(check_device());
+    if (!edges_out) return bad("edges_out must not be NULL");
+    *edges_out = 0;
+    if (vertices < 1 || edges < 0) return bad("need vertices >= 1 and edges >= 0");
+    if (edges >= (int64_t)INT32_MAX) {
+        set_error("edge lists of 2^31 or more edges are not supported");
+        return TRAV_ERR_OVERFLOW_INT32;
+    }
+    if (segment < 0) return bad("segment must be >= 0");
+    if (mem != TRAV_MEM_HOST && mem != TRAV_MEM_DEVICE) return bad("mem must be TRAV_MEM_HOST or TRAV_MEM_DEVICE");
+    if (edges == 0) return TRAV_OK;
+    if (!src || !dst || !w) return bad("src, dst and w must hold `edges` entries");
+    if (mem == TRAV_MEM_DEVICE && (!is_device_ptr(src) || !is_device_ptr(dst) || !is_device_ptr(w)))
+        return bad("src, dst and w must be device arrays (mem = TRAV_MEM_DEVICE)");
+    TRY_CUDA(cudaDeviceSynchronize());
+    DevTmp<int32_t> ds, dd;
+    DevTmp<float> dw;
+    int32_t *s = src, *d = dst;
+    float *ww = w;
+    const size_t bi = sizeof(int32_t) * (size_t)edges, bf = sizeof(float) * (size_t)edges;
+    if (mem == TRAV_MEM_HOST) {
+        TRY_CUDA(cudaMalloc(&ds.p, bi));
+        TRY_CUDA(cudaMalloc(&dd.p, bi));
+        TRY_CUDA(cudaMalloc(&dw.p, bf));
+        TRY_CUDA(cudaMemcpy(ds.p, src, bi, cudaMemcpyHostToDevice));
+        TRY_CUDA(cudaMemcpy(dd.p, dst, bi, cudaMemcpyHostToDevice));
+        TRY_CUDA(cudaMemcpy(dw.p, w, bf, cudaMemcpyHostToDevice));
+        s = ds.p, d = dd.p, ww = dw.p;
+    }
+    TRY(validate_edges(vertices, edges, s, d, ww, 0));
+    TRY(el_optimize_device(s, d, ww, edges, segment, edges_out, 0));
+    if (mem == TRAV_MEM_HOST && *edges_out > 0) {
+        const size_t n = (size_t)*edges_out;
+        TRY_CUDA(cudaMemcpy(src, s, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+        TRY_CUDA(cudaMemcpy(dst, d, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+        TRY_CUDA(cudaMemcpy(w, ww, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    }
+    return TRAV_OK;
+}
+
+int trav_el_gpu_transactions(const int32_t *src, const int32_t *dst, int32_t vertices, int64_t edges,
+                             int32_t elem_size, int32_t mem, int64_t *count)
+{
+    TRY(check_device());
+    if (!count) return bad("count must not be NULL");
+    *count = 0;
+    if (vertices < 1 || edges < 0 || elem_size < 1) return bad("need vertices >= 1, edges >= 0 and elem_size >= 1");
+    if (mem != TRAV_MEM_HOST && mem != TRAV_MEM_DEVICE) return bad("mem must be TRAV_MEM_HOST or TRAV_MEM_DEVICE");
+    if (edges == 0) return TRAV_OK;
+    if (!src || !dst) return bad("src and dst must hold `edges` entries");
+    if (mem == TRAV_MEM_DEVICE && (!is_device_ptr(src) || !is_device_ptr(dst)))
+        return bad("src and dst must be device arrays (mem = TRAV_MEM_DEVICE)");
+    TRY_CUDA(cudaDeviceSynchronize());
+    DevTmp<int32_t> ds, dd;
+    const int32_t *s = src, *d = dst;
+    if (mem == TRAV_MEM_HOST) {
+        const size_t bi = sizeof(int32_t) * (size_t)edges;
+        TRY_CUDA(cudaMalloc(&ds.p, bi));
+        TRY_CUDA(cudaMalloc(&dd.p, bi));
+        TRY_CUDA(cudaMemcpy(ds.p, src, bi, cudaMemcpyHostToDevice));
+        TRY_CUDA(cudaMemcpy(dd.p, dst, bi, cudaMemcpyHostToDevice));
+        s = ds.p, d = dd.p;
+    }
+    TRY(validate_edges(vertices, edges, s, d, nullptr, 0));
+    return el_transactions_device(s, d, edges, elem_size, count, 0);
+}
+
 int trav_graph_set_capture(trav_graph *g, int32_t on)
 {
     if (!g) return bad("graph handle is NULL");

@@ -224,6 +224,12 @@ int rmat_device(int scale, int avg, int a, int b, int c, int d, uint32_t seed, i
 int validate_edges(int32_t V, int64_t E, const int32_t *d_src, const int32_t *d_dst, const float *d_w,
                    cudaStream_t st);
 
+// el_optimize.cu
+int el_optimize_device(int32_t *src, int32_t *dst, float *w, int64_t E, int32_t segment, int64_t *E_out,
+                       cudaStream_t st);
+int el_transactions_device(const int32_t *src, const int32_t *dst, int64_t E, int32_t elem, int64_t *count,
+                           cudaStream_t st);
+
 // traverse.cu
 int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_t st);
 void workspace_free(Workspace *ws);

@@ -14,6 +14,7 @@
 // message.
 #pragma once
 
+#include <climits>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -129,6 +130,37 @@ struct GraphGenerationAPI {
                 g.src_ids[(size_t)k] = o2n[(size_t)r];
                 g.dst_ids[(size_t)k] = o2n[(size_t)adj[(size_t)k]];
             }
+    }
+};
+
+// GraphOptimizationAPI::optimize_graph_for_GPU and
+// check_gpu_memory_transactions_count
+// (include/test/optimization/graph_optimization_API.hpp:173-266), run on the
+// device: loops and repeated arcs are removed and edges grouped by segments of
+// l2_bytes / elem_size vertices (the B200's 126 MB L2 by default, where the
+// reference names Kepler's or Pascal's).
+struct GraphOptimizationAPI {
+    static constexpr long long kB200L2Bytes = 126LL * 1024 * 1024;
+
+    static void optimize_graph_for_GPU(EdgesList &g, int elem_size, long long l2_bytes = kB200L2Bytes)
+    {
+        int64_t n = 0;
+        const long long seg = l2_bytes / (elem_size > 0 ? elem_size : 1);
+        check(trav_el_optimize(g.src_ids.data(), g.dst_ids.data(), g.weights.data(), g.vertices_count,
+                               g.get_edges_count(), (int32_t)(seg < INT32_MAX ? seg : INT32_MAX), TRAV_MEM_HOST, &n),
+              "trav_el_optimize");
+        g.src_ids.resize((size_t)n);
+        g.dst_ids.resize((size_t)n);
+        g.weights.resize((size_t)n);
+    }
+
+    static long long check_gpu_memory_transactions_count(const EdgesList &g, int elem_size)
+    {
+        int64_t n = 0;
+        check(trav_el_gpu_transactions(g.src_ids.data(), g.dst_ids.data(), g.vertices_count, g.get_edges_count(),
+                                       elem_size, TRAV_MEM_HOST, &n),
+              "trav_el_gpu_transactions");
+        return (long long)n;
     }
 };
 

@@ -50,6 +50,7 @@ EXPORTS = [
     "trav_bfs_csr_noalloc", "trav_last_phase_log", "trav_mlp_loss_grad", "trav_mlp_train", "trav_set_plan",
     "trav_last_decisions", "trav_set_grid", "trav_batch_create", "trav_batch_free", "trav_batch_run",
     "trav_batch_autotune", "trav_batch_set_shape", "trav_batch_get_shape", "trav_graph_set_capture",
+    "trav_el_optimize", "trav_el_gpu_transactions",
 ]
 
 
@@ -114,6 +115,8 @@ def lib():
         L.trav_mlp_set.argtypes = [vp, i32, vp, i32]
         L.trav_set_grid.argtypes = [vp, i32, i32, C.POINTER(i32)]
         L.trav_graph_set_capture.argtypes = [vp, i32]
+        L.trav_el_optimize.argtypes = [vp, vp, vp, i32, i64, i32, i32, C.POINTER(i64)]
+        L.trav_el_gpu_transactions.argtypes = [vp, vp, i32, i64, i32, i32, C.POINTER(i64)]
         L.trav_batch_create.argtypes = [C.POINTER(vp), i32, C.POINTER(vp)]
         L.trav_batch_free.argtypes = [vp]
         L.trav_batch_free.restype = None
@@ -482,3 +485,20 @@ class Batch:
     def shape(self, value):
         s = BatchShape(*value)
         _check(lib().trav_batch_set_shape(self._h, C.byref(s)))
+
+
+def el_optimize(src, dst, w, vertices: int, segment: int = 0):
+    """The optimisation pass, in place on int32 src / dst and float32 w (numpy arrays or CUDA tensors); returns
+    the new edge count (the first that many entries hold the result)."""
+    n = C.c_int64(0)
+    mem = MEM_DEVICE if _is_cuda(src) else MEM_HOST
+    _check(lib().trav_el_optimize(_ptr(src), _ptr(dst), _ptr(w), vertices, len(src), segment, mem, C.byref(n)))
+    return n.value
+
+
+def el_gpu_transactions(src, dst, vertices: int, elem_size: int = 4) -> int:
+    """Memory transactions of an edge-per-thread sweep over src / dst (numpy arrays or CUDA tensors)."""
+    n = C.c_int64(0)
+    mem = MEM_DEVICE if _is_cuda(src) else MEM_HOST
+    _check(lib().trav_el_gpu_transactions(_ptr(src), _ptr(dst), vertices, len(src), elem_size, mem, C.byref(n)))
+    return n.value

@@ -83,6 +83,28 @@ def digest(*arrays):
     return h.hexdigest()
 
 
+def optimize_fixture():
+    """An edge list with loops, repeated arcs (some with equal weights), zero weights and ids spread over four
+    of the reference's CPU cache segments (65,536 vertices at elem_size 4); the reference's
+    optimize_graph_for_CPU result and check_gpu_memory_transactions_count before and after."""
+    rng = np.random.default_rng(17)
+    V, E = 250000, 20011
+    s = rng.integers(0, V, E).astype(np.int32)
+    d = rng.integers(0, V, E).astype(np.int32)
+    w = (rng.integers(0, 8, E) / 8).astype(np.float32)
+    s[:300] = d[:300]                          # loops
+    s[300:1300], d[300:1300] = s[1300:2300], d[1300:2300]  # repeated arcs
+    g = O.RefGraph.edges_list(V, s, d, w)
+    before = {str(k): g.gpu_transactions(k) for k in (4, 8)}
+    n = g.optimize_for_cpu(4)
+    os_, od, ow = g.export_el()
+    after = {str(k): g.gpu_transactions(k) for k in (4, 8)}
+    g.free()
+    np.savez_compressed(os.path.join(HERE, "el_optimize.npz"), src=s, dst=d, w=w, ref_src=os_, ref_dst=od, ref_w=ow)
+    return {"V": V, "E": E, "E_after": int(n), "segment": 262144 // 4, "transactions_before": before,
+            "transactions_after_reference_order": after}
+
+
 def main():
     if not O.ref_available():
         raise SystemExit("oracle/_ref/libtrav_ref.so is missing: run oracle/build_ref.sh first")
@@ -141,6 +163,9 @@ def main():
     with open(os.path.join(HERE, "adj_small.bin"), "wb") as f:
         f.write(adj)
     meta["files"] = {"V": V, "src": s.tolist(), "dst": d.tolist(), "w": w.tolist()}
+
+    # --- graph optimisation pass: the reference's optimize_graph_for_CPU and its transaction count
+    meta["optimize"] = optimize_fixture()
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(meta, f, indent=1, sort_keys=True)
     print("wrote golden fixtures:", sorted(os.listdir(HERE)))

@@ -1,6 +1,7 @@
 """The CPU oracle pinned against the reference's golden vectors (and the live reference build when present)."""
 import ctypes
 import hashlib
+import os
 
 import numpy as np
 import pytest
@@ -169,3 +170,52 @@ def test_el_file_bytes_layout():
     V = int.from_bytes(b[1:5], "little")
     E = int.from_bytes(b[5:13], "little")
     assert (V, E) == (6, 6)
+
+
+def test_el_optimize_matches_reference_fixture(golden):
+    """The optimisation pass restatement against the reference's optimize_graph_for_CPU output (fixture)."""
+    f = np.load(os.path.join(os.path.dirname(__file__), "golden", "el_optimize.npz"))
+    meta = golden[0]["optimize"]
+    seg = meta["segment"]
+    s, d, w = O.el_optimize(f["src"], f["dst"], f["w"], segment=seg)
+    assert len(s) == meta["E_after"] == len(f["ref_src"])
+    # same arcs and weights (the reference's std::sort leaves the order inside a segment pair open)
+    mine = sorted(zip(s.tolist(), d.tolist(), w.tolist()))
+    ref = sorted(zip(f["ref_src"].tolist(), f["ref_dst"].tolist(), f["ref_w"].tolist()))
+    assert mine == ref
+    # both orders group edges by (src // segment, dst // segment)
+    for a, b in ((s, d), (f["ref_src"], f["ref_dst"])):
+        key = (a // seg).astype(np.int64) * (1 << 20) + (b // seg)
+        assert np.all(np.diff(key) >= 0)
+    # inside a group, the restatement keeps (src, dst, w) order
+    key = (s // seg).astype(np.int64) * (1 << 20) + (d // seg)
+    order = np.lexsort((w, d, s, key))
+    assert np.array_equal(order, np.arange(len(s)))
+    assert len(set(zip(s.tolist(), d.tolist()))) == len(s) and not np.any(s == d)
+
+
+def test_gpu_transactions_matches_reference_fixture(golden):
+    f = np.load(os.path.join(os.path.dirname(__file__), "golden", "el_optimize.npz"))
+    meta = golden[0]["optimize"]
+    for k, want in meta["transactions_before"].items():
+        assert O.gpu_transactions(f["src"], f["dst"], int(k)) == want
+    for k, want in meta["transactions_after_reference_order"].items():
+        assert O.gpu_transactions(f["ref_src"], f["ref_dst"], int(k)) == want
+
+
+def test_el_optimize_live_reference_small_segments():
+    if not O.ref_available():
+        pytest.skip("reference build not present")
+    rng = np.random.default_rng(5)
+    for V, E in ((70000, 3001), (140000, 9000), (10, 40), (5, 31)):
+        s = rng.integers(0, V, E).astype(np.int32)
+        d = rng.integers(0, V, E).astype(np.int32)
+        w = (rng.integers(0, 3, E) / 2).astype(np.float32)
+        g = O.RefGraph.edges_list(V, s, d, w)
+        assert O.gpu_transactions(s, d, 4) == g.gpu_transactions(4)
+        n = g.optimize_for_cpu(4)
+        rs, rd, rw = g.export_el()
+        ms, md, mw = O.el_optimize(s, d, w, segment=65536)
+        assert n == len(ms)
+        assert sorted(zip(ms.tolist(), md.tolist(), mw.tolist())) == sorted(zip(rs.tolist(), rd.tolist(), rw.tolist()))
+        g.free()
