@@ -86,7 +86,7 @@ __host__ __device__ inline Feat sssp_features(int steps, unsigned long long far_
     f.x[6] = fslog2p1(mw / d) / 8.0f;
     f.x[7] = fslog2p1(gap / mw) / 8.0f;
     f.x[8] = flog2p1((double)thr / mw) / 16.0f;
-    f.x[9] = flog2p1((double)E) / 32.0f;
+    f.x[9] = (flog2p1((double)E) - 16.0f) / 12.0f;  // about 0 at 2^16 edges, 1 at 2^28
     return f;
 }
 

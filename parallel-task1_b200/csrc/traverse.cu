@@ -47,6 +47,53 @@ __device__ __forceinline__ int ld_relaxed_int(const int *p)
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
 
+// L2 eviction priorities.  The adjacency and weight arrays stream through
+// once per phase while the distance words (8 B per vertex) are gathered at
+// random over and over: streamed lines are marked evict-first and gathered
+// ones evict-last, so the stream does not push the distances out of L2.
+#ifndef TRAV_L2HINT
+#define TRAV_L2HINT 1
+#endif
+__device__ __forceinline__ unsigned long long l2_policy_evict_first()
+{
+    unsigned long long pol;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+__device__ __forceinline__ unsigned long long l2_policy_evict_last()
+{
+    unsigned long long pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+// read-only stream load (non-coherent path), evict-first in L2
+__device__ __forceinline__ int ld_stream(const int *p)
+{
+#if TRAV_L2HINT
+    int v;
+    asm("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(l2_policy_evict_first()));
+    return v;
+#else
+    return __ldg(p);
+#endif
+}
+
+__device__ __forceinline__ float ld_stream(const float *p) { return __int_as_float(ld_stream(reinterpret_cast<const int *>(p))); }
+
+// gather of a mutable word at L2 (bypassing L1), evict-last in L2
+__device__ __forceinline__ unsigned long long ld_gather(const unsigned long long *p)
+{
+#if TRAV_L2HINT
+    unsigned long long v;
+    asm volatile("ld.global.cg.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(l2_policy_evict_last()));
+    return v;
+#else
+    return __ldcg(p);
+#endif
+}
+
 __device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned *p)
 {
     unsigned v;
@@ -732,13 +779,26 @@ struct BfsPush {
 
     __device__ __forceinline__ float begin(int) const { return 0.0f; }
 
-    __device__ __forceinline__ void visit_batch(const int (&)[kBatch], const float (&)[kBatch], const int (&e)[kBatch],
-                                                const bool (&ok)[kBatch], Pusher &p) const
+    __device__ __forceinline__ void load_at(const int (&e)[kBatch], const bool (&ok)[kBatch], int (&v)[kBatch],
+                                            float (&)[kBatch]) const
+    {
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) v[j] = ok[j] ? ld_stream(&a->out_adj[e[j]]) : 0;
+    }
+
+    __device__ __forceinline__ void visit_batch(const int (&)[kBatch], const float (&du)[kBatch],
+                                                const int (&e)[kBatch], const bool (&ok)[kBatch], Pusher &p) const
     {
         int v[kBatch];
+        float w[kBatch];
+        load_at(e, ok, v, w);
+        visit_loaded(du, v, w, ok, p);
+    }
+
+    __device__ __forceinline__ void visit_loaded(const float (&)[kBatch], const int (&v)[kBatch],
+                                                 const float (&)[kBatch], const bool (&ok)[kBatch], Pusher &p) const
+    {
         unsigned word[kBatch];
-#pragma unroll
-        for (int j = 0; j < kBatch; j++) v[j] = ok[j] ? __ldg(&a->out_adj[e[j]]) : 0;
 #pragma unroll
         for (int j = 0; j < kBatch; j++) word[j] = ok[j] ? __ldcg(&a->visited[v[j] >> 5]) : ~0u;
         bool fresh[kBatch];
@@ -800,23 +860,34 @@ struct SsspPush {
 
     __device__ __forceinline__ float begin(int u) const { return dist_of(__ldcg(&a->dist[u])); }
 
+    __device__ __forceinline__ void load_at(const int (&e)[kBatch], const bool (&ok)[kBatch], int (&v)[kBatch],
+                                            float (&w)[kBatch]) const
+    {
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) {
+            v[j] = ok[j] ? ld_stream(&a->out_adj[e[j]]) : 0;
+            w[j] = ok[j] ? ld_stream(&a->out_w[e[j]]) : 0.0f;
+        }
+    }
+
     __device__ __forceinline__ void visit_batch(const int (&)[kBatch], const float (&du)[kBatch],
                                                 const int (&e)[kBatch], const bool (&ok)[kBatch], Pusher &p) const
     {
         int v[kBatch];
+        float w[kBatch];
+        load_at(e, ok, v, w);
+        visit_loaded(du, v, w, ok, p);
+    }
+
+    __device__ __forceinline__ void visit_loaded(const float (&du)[kBatch], const int (&v)[kBatch],
+                                                 const float (&w)[kBatch], const bool (&ok)[kBatch], Pusher &p) const
+    {
         float nd[kBatch];
         unsigned long long cur[kBatch];
 #pragma unroll
-        for (int j = 0; j < kBatch; j++) {
-            v[j] = 0;
-            nd[j] = 0.0f;
-            if (ok[j]) {
-                v[j] = __ldg(&a->out_adj[e[j]]);
-                nd[j] = __fadd_rn(du[j], __ldg(&a->out_w[e[j]]));  // one rounded add, as sssp.hpp:56
-            }
-        }
+        for (int j = 0; j < kBatch; j++) nd[j] = ok[j] ? __fadd_rn(du[j], w[j]) : 0.0f;  // one rounded add, as sssp.hpp:56
 #pragma unroll
-        for (int j = 0; j < kBatch; j++) cur[j] = ok[j] ? __ldcg(&a->dist[v[j]]) : 0ull;
+        for (int j = 0; j < kBatch; j++) cur[j] = ok[j] ? ld_gather(&a->dist[v[j]]) : 0ull;
         bool light[kBatch], heavy[kBatch], far[kBatch];
 #pragma unroll
         for (int j = 0; j < kBatch; j++) {
@@ -987,7 +1058,7 @@ __device__ __forceinline__ int bfs_query(const TravArgs &a, QueryShared &sh, int
                     for (int kk = kb + lane; kk - lane < ke; kk += 32) {
                         bool h = false;
                         if (kk < ke) {
-                            const int u = __ldg(&a.in_adj[kk]);
+                            const int u = ld_stream(&a.in_adj[kk]);
                             h = (fc[u >> 5] >> (u & 31)) & 1u;
                         }
                         if (__any_sync(kFull, h)) {
@@ -1003,7 +1074,7 @@ __device__ __forceinline__ int bfs_query(const TravArgs &a, QueryShared &sh, int
                 // short in-rows: one lane each
                 if (cand) {
                     for (; k < kend; k++) {
-                        const int u = __ldg(&a.in_adj[k]);
+                        const int u = ld_stream(&a.in_adj[k]);
                         if ((fc[u >> 5] >> (u & 31)) & 1u) { found = true; break; }
                     }
                 }
