@@ -167,6 +167,7 @@ int build_queries(trav_batch *b, const trav_query *qs, int32_t n, std::vector<Ba
         d.V = g->g.V;
         d.E = g->g.E;
         d.mean_w = g->g.mean_w;
+        d.max_deg = g->g.max_out_degree;
         d.kind = q.kind;
         d.source = g->new_of_old[(size_t)q.source];
         d.out = q.out;

@@ -67,10 +67,12 @@ __host__ __device__ inline Feat bfs_features(int step, unsigned long long nf, un
 // share of the vertices, the gap from the current bound to the nearest far
 // entry and the bound itself in units of delta and of the mean edge weight,
 // mean degree, the mean edge weight in units of delta (how many buckets one
-// edge spans), and the graph's size: whether wide buckets pay depends on it,
+// edge spans), the degree skew (largest out-degree over the mean: wide
+// buckets pay on skewed graphs, whose hubs settle early, and cost re-relaxation
+// on even ones), and the graph's size: whether wide buckets pay depends on it,
 // since they trade fewer rounds (latency) for more re-relaxation (work).
 __host__ __device__ inline Feat sssp_features(int steps, unsigned long long far_len, float min_far, float thr,
-                                              float delta, int V, long long E, int buckets, float mean_w)
+                                              float delta, int V, long long E, int buckets, float mean_w, int max_deg)
 {
     Feat f;
     const double d = delta > 0 ? (double)delta : 1.0;
@@ -85,7 +87,7 @@ __host__ __device__ inline Feat sssp_features(int steps, unsigned long long far_
     f.x[5] = flog2p1((double)buckets) / 16.0f;
     f.x[6] = fslog2p1(mw / d) / 8.0f;
     f.x[7] = fslog2p1(gap / mw) / 8.0f;
-    f.x[8] = flog2p1((double)thr / mw) / 16.0f;
+    f.x[8] = flog2p1((double)max_deg / ((double)E / v + 1.0)) / 16.0f;
     f.x[9] = (flog2p1((double)E) - 16.0f) / 12.0f;  // about 0 at 2^16 edges, 1 at 2^28
     return f;
 }

@@ -158,6 +158,7 @@ struct TravArgs {
     // SSSP options
     float delta;           // +inf = Bellman-Ford
     float mean_w;          // mean edge weight of the graph
+    int32_t max_deg;       // largest out-degree of the graph
     // output (original ids); nullptr = leave results in `value`
     void *out;
     int32_t out_kind;      // 0 = int32 levels, 1 = float distances, 2 = uint8 reached flags
@@ -187,6 +188,7 @@ struct BatchQuery {
     int32_t source;         // new id
     float delta;            // SSSP bucket width (+inf = Bellman-Ford)
     float mean_w;           // mean edge weight
+    int32_t max_deg;        // largest out-degree
 };
 
 // Scratch of one team of a batch launch, sized for the batch's largest graph.

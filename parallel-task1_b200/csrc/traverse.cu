@@ -1302,7 +1302,8 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, in
         } else if (far_len > 0) {
             // open the next bucket (skipping empty ones): bound = max(old, min far) + width
             if (threadIdx.x < 32) {
-                const Feat f = sssp_features(steps, far_len, __int_as_float(min_far), thr, a.delta, a.V, a.E, buckets, a.mean_w);
+                const Feat f = sssp_features(steps, far_len, __int_as_float(min_far), thr, a.delta, a.V, a.E, buckets, a.mean_w,
+                                             a.max_deg);
                 int o = 0;
                 if (a.mlp) o = mlp_argmax_warp<kSsspOut>(sh.mlp, f);
                 const int forced = planned(a, buckets - 1);
@@ -1460,6 +1461,7 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) batch_persistent
             a.force_dir = -1;
             a.delta = q.delta;
             a.mean_w = q.mean_w;
+            a.max_deg = q.max_deg;
             a.out_kind = 1;
             ph = sssp_query(a, sh, ph);
         }
@@ -1768,6 +1770,7 @@ static TravArgs make_args(const DevGraph &g, Workspace *ws)
     a.chunks1 = ws->chunks[1];
     a.timeout_ns = 10ull * 1000000000ull;
     a.mean_w = g.mean_w;
+    a.max_deg = g.max_out_degree;
     a.cta0 = 0;
     a.ctas = 0;  // set at launch
     a.small_deg = ws->small_deg;
