@@ -1071,11 +1071,15 @@ __device__ __forceinline__ int bfs_query(const TravArgs &a, QueryShared &sh, int
                         cand = false;
                     }
                 }
-                // short in-rows: one lane each
+                // short in-rows: one lane each, four parents per probe (independent loads)
                 if (cand) {
-                    for (; k < kend; k++) {
-                        const int u = ld_stream(&a.in_adj[k]);
-                        if ((fc[u >> 5] >> (u & 31)) & 1u) { found = true; break; }
+                    for (; k < kend && !found; k += 4) {
+                        int u[4];
+#pragma unroll
+                        for (int i = 0; i < 4; i++) u[i] = k + i < kend ? ld_stream(&a.in_adj[k + i]) : -1;
+#pragma unroll
+                        for (int i = 0; i < 4; i++)
+                            if (u[i] >= 0 && ((fc[u[i] >> 5] >> (u[i] & 31)) & 1u)) found = true;
                     }
                 }
                 const unsigned m = __ballot_sync(kFull, found);
