@@ -3,9 +3,10 @@
 Workload (default): RMAT scale 23 (V = 8,388,608), edge factor 32 (268,435,456 directed edges before the
 self-loop drop), a/b/c/d = 57/19/19/5, fp32 weights rand_r/RAND_MAX, seed 1, self-loops dropped; 64 seeded
 sources of nonzero out-degree.  One step = BFS (Beamer alpha 15 / beta 18) from each of the 64 sources plus
-SSSP (delta-stepping, delta 0.1) from each of them.  TEPS = edges in the graph / traversal time (the
-reference's convention), summed over traversals.  The graph (2.2 GB of CSR + CSC) is larger than the 126 MB
-L2, so no flush runs between steps.
+SSSP (delta-stepping, delta 0.1) from each of them, the 128 queries run as one batched persistent launch
+(teams of CTAs, one query each at a time; shape autotuned outside the timed region).  TEPS = edges in the
+graph / traversal time (the reference's convention), summed over traversals.  The graph (2.2 GB of CSR + CSC)
+is larger than the 126 MB L2, so no flush runs between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--scale S] [--ef F]
 
@@ -152,16 +153,21 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/traffic.txt), if any."""
+def ncu_traffic(kernel: str, queries: int = 1):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/traffic.txt), if any.  An entry
+    with bytes_per_query (a capture of fewer queries than the bench's launch) is scaled to `queries`."""
     p = os.path.join(ROOT, "profiles", "traffic.txt")
     if not os.path.exists(p):
         return None
     with open(p) as f:
         for line in f:
             kv = dict(x.split("=", 1) for x in line.split() if "=" in x)
-            if kv.get("kernel") == kernel and "bytes_per_launch" in kv:
+            if kv.get("kernel") != kernel:
+                continue
+            if "bytes_per_launch" in kv:
                 return float(kv["bytes_per_launch"])
+            if "bytes_per_query" in kv:
+                return float(kv["bytes_per_query"]) * queries
     return None
 
 
@@ -291,17 +297,25 @@ def run_ours(a):
     primary = schedules[0]
     names = {T.SCHEDULE_PLAIN: "plain", T.SCHEDULE_LEARNED: "learned"}
 
+    # One step = BFS and SSSP from every source.  The 2n queries run concurrently in one batched persistent
+    # launch (trav_batch_run): teams of CTAs each run one query at a time, so the latency-bound tails of one
+    # query overlap the work of others.  The launch shape is autotuned once per schedule, outside the timed region.
+    import ctypes
+
+    batch = T.Batch([g])
+    queries = {sched: [(0, 0, int(s), 0.0, sched, lv_dev[i]) for i, s in enumerate(sources)]
+               + [(0, 1, int(s), a.delta, sched, di_dev[i]) for i, s in enumerate(sources)]
+               for sched in schedules}
+
     def step(sched, record):
-        g.bfs(sources, out=lv_dev, schedule=sched)
+        ms = batch.run(queries[sched])
         if record is not None:
-            record["bfs"].extend(g.last_batch_ms().tolist())
-        g.sssp(sources, out=di_dev, delta=a.delta, schedule=sched)
-        if record is not None:
-            record["sssp"].extend(g.last_batch_ms().tolist())
+            record.append(ms)
 
     # Each schedule: algorithmic bytes per traversal measured once per source outside the timed region (the
     # SSSP count is schedule-independent; the BFS count follows the direction trace, which is deterministic),
-    # W warm-up steps, then K timed steps bracketed by a barrier and a device synchronisation.
+    # the shape autotuned, W warm-up steps, then K timed steps bracketed by a barrier and a device
+    # synchronisation; the step time is the device time of its launch (CUDA events around it).
     runs = {}
     clk = None
     for sched in schedules:
@@ -311,6 +325,7 @@ def run_ours(a):
             bfs_bytes.append(g.last_stats().algorithmic_bytes)
             g.sssp([s], out=di_dev[:1], delta=a.delta, schedule=sched)
             sssp_bytes.append(g.last_stats().algorithmic_bytes)
+        shape = batch.autotune(queries[sched], reps=1)
         for _ in range(a.warmup):
             step(sched, None)
         if world > 1:
@@ -319,20 +334,16 @@ def run_ours(a):
         clocks = ClockSampler(local) if sched == primary else None
         if clocks:
             clocks.start()
-        rec = {"bfs": [], "sssp": []}
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
+        rec = []
         for _ in range(a.steps):
             step(sched, rec)
-        e1.record(stream)
         torch.cuda.synchronize()
         if clocks:
             clk = clocks.stop()
         if world > 1:
             dist.barrier()
-        ms_max = max_over_ranks(e0.elapsed_time(e1), world, dev)
-        runs[sched] = dict(ms=ms_max, rec=rec, bfs_bytes=bfs_bytes, sssp_bytes=sssp_bytes,
+        ms_max = max_over_ranks(sum(rec), world, dev)
+        runs[sched] = dict(ms=ms_max, rec=rec, bfs_bytes=bfs_bytes, sssp_bytes=sssp_bytes, shape=shape,
                            lv=lv_dev.cpu().numpy(), di=di_dev.cpu().numpy())
     traversals = 2 * n * a.steps
     value = job_gteps(traversals, E, world, runs[primary]["ms"] / 1e3)
@@ -340,49 +351,67 @@ def run_ours(a):
         assert np.array_equal(runs[0]["lv"], runs[1]["lv"])
         assert np.array_equal(runs[0]["di"].view(np.uint32), runs[1]["di"].view(np.uint32))
 
-    # e2e through the public API with pinned host buffers: per step, H2D of the source ids (inside the call)
-    # and D2H of every level / distance array, timed on the host clock around the synchronous calls
+    # the same step as one persistent launch per query (the single-query API), for comparison
+    seq_ms = []
+    for rep in range(3):
+        g.bfs(sources, out=lv_dev, schedule=primary)
+        t = float(np.sum(g.last_batch_ms()))
+        g.sssp(sources, out=di_dev, delta=a.delta, schedule=primary)
+        t += float(np.sum(g.last_batch_ms()))
+        if rep:
+            seq_ms.append(t)
+    seq_ms = min(seq_ms)
+    assert np.array_equal(runs[primary]["lv"], lv_dev.cpu().numpy())
+    assert np.array_equal(runs[primary]["di"].view(np.uint32), di_dev.cpu().numpy().view(np.uint32))
+
+    # e2e through the public API with pinned host buffers: per step, the query descriptors (source ids inside)
+    # go H2D in the call and every level / distance array comes back D2H.  The step runs as four launches of a
+    # quarter of the queries; each quarter's results are copied on a second stream while the next quarter runs.
+    # Timed on the host clock.
     lv_host = torch.empty((n, V), dtype=torch.int32).pin_memory()
     di_host = torch.empty((n, V), dtype=torch.float32).pin_memory()
-    src_host = torch.from_numpy(sources).pin_memory()
-    lvn, din = lv_host.numpy(), di_host.numpy()
-    g.set_stream(None)
+    cs = torch.cuda.Stream()
+    parts = 4
+    cut = [round(i * n / parts) for i in range(parts + 1)]
+    chunks = [queries[primary][cut[i]:cut[i + 1]] + queries[primary][n + cut[i]:n + cut[i + 1]] for i in range(parts)]
 
     def e2e_step():
-        s = src_host.numpy()
-        g.bfs(s, out=lvn, schedule=primary)
-        g.sssp(s, out=din, delta=a.delta, schedule=primary)
+        for i, q in enumerate(chunks):
+            batch.run(q)
+            with torch.cuda.stream(cs):
+                lv_host[cut[i]:cut[i + 1]].copy_(lv_dev[cut[i]:cut[i + 1]], non_blocking=True)
+                di_host[cut[i]:cut[i + 1]].copy_(di_dev[cut[i]:cut[i + 1]], non_blocking=True)
+        cs.synchronize()
 
     for _ in range(max(1, min(a.warmup, 2))):
         e2e_step()
     if world > 1:
         dist.barrier()
+    torch.cuda.synchronize()
     h0 = time.perf_counter()
     for _ in range(a.steps):
         e2e_step()
     h1 = time.perf_counter()
     e2e_value = job_gteps(traversals, E, world, max_over_ranks(h1 - h0, world, dev))
+    h2d = len(queries[primary]) * ctypes.sizeof(T.Query)
 
-    # parity spot check of the timed outputs against the host-path outputs (same kernels, same inputs)
-    assert np.array_equal(runs[primary]["lv"], lvn)
-    assert np.array_equal(runs[primary]["di"].view(np.uint32), din.view(np.uint32))
+    # parity spot check of the timed outputs against the host copies (same kernels, same inputs)
+    assert np.array_equal(runs[primary]["lv"], lv_host.numpy())
+    assert np.array_equal(runs[primary]["di"].view(np.uint32), di_host.numpy().view(np.uint32))
+    batch.close()
 
-    # roofline of the dominant kernel of the primary schedule (largest share of the timed device time)
+    # roofline of the timed kernel: all queries' algorithmic bytes over the launch's device time
     rec = runs[primary]["rec"]
-    tot_bfs, tot_sssp = sum(rec["bfs"]), sum(rec["sssp"])
-    kind = "sssp" if tot_sssp >= tot_bfs else "bfs"
-    launches = rec[kind]
-    mean_ms = statistics.mean(launches)
-    mean_bytes = statistics.mean(runs[primary]["sssp_bytes" if kind == "sssp" else "bfs_bytes"])
-    achieved = mean_bytes / (mean_ms / 1e3) / 1e9
+    mean_ms = statistics.mean(rec)
+    launch_bytes = float(sum(runs[primary]["sssp_bytes"]) + sum(runs[primary]["bfs_bytes"]))
+    achieved = launch_bytes / (mean_ms / 1e3) / 1e9
     peak, peak_src = measured_peaks()
-    kname = "sssp_persistent" if kind == "sssp" else "bfs_persistent"
-    traffic = ncu_traffic(kname)
+    kname = "batch_persistent"
+    traffic = ncu_traffic(kname, queries=len(queries[primary]))
 
     if rank == 0:
-        gteps = lambda ms_list: n * a.steps * E / (sum(ms_list) / 1e3) / 1e9  # noqa: E731
         per = {names[k]: {"gteps": job_gteps(traversals, E, world, r["ms"] / 1e3), "ms_per_step": r["ms"] / a.steps,
-                          "bfs_gteps": gteps(r["rec"]["bfs"]), "sssp_gteps": gteps(r["rec"]["sssp"])}
+                          "shape": {"team_ctas": r["shape"][0], "small_deg": r["shape"][1], "item": r["shape"][2]}}
                for k, r in runs.items()}
         line = {
             "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": a.steps,
@@ -391,17 +420,21 @@ def run_ours(a):
             "data": "synthetic (seeded RMAT generated on the device)",
             "config": {"workload": workload_name(a), "scale": a.scale, "edge_factor": a.ef, "vertices": V,
                        "edges": E, "sources": n, "schedule": names[primary], "l2": "inputs larger than L2 (no flush)",
+                       "execution": "each step's 2n queries in one batched persistent launch (autotuned teams)",
                        "parallelism": f"replicas x{world}"},
-            "bfs_gteps": per[names[primary]]["bfs_gteps"], "sssp_gteps": per[names[primary]]["sssp_gteps"],
             "schedules": per,
+            "sequential_launches": {"gteps": job_gteps(2 * n, E, 1, seq_ms / 1e3), "ms_per_step": seq_ms,
+                                    "note": "the same step as one persistent launch per query, primary schedule"},
             "learned_over_plain": (per["learned"]["gteps"] / per["plain"]["gteps"]) if "learned" in per else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": kname,
                          "peak_source": peak_src,
-                         "algorithmic_bytes_per_launch": mean_bytes, "mean_launch_ms": mean_ms},
-            "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 2 * 4 * n,
-                    "d2h_bytes_per_step": 2 * 4 * n * V, "timing": "host clock around synchronous C-ABI calls"},
-            "gpu_launches": traversals,
+                         "algorithmic_bytes_per_launch": launch_bytes, "mean_launch_ms": mean_ms,
+                         "queries_per_launch": len(queries[primary])},
+            "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": 2 * 4 * n * V,
+                    "timing": "host clock around the batched C-ABI calls and the overlapped result copies"},
+            "gpu_launches": a.steps,
             "ingest_s": ingest_s,
             "clocks": clk,
         }

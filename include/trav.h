@@ -323,7 +323,9 @@ int trav_batch_create(trav_graph *const *graphs, int32_t n, trav_batch **out);
 void trav_batch_free(trav_batch *b);
 
 /* Run n queries in one launch and wait for it; *device_ms (may be NULL)
- * receives the launch's device time. */
+ * receives the launch's device time.  Every team holds scratch for the
+ * batch's largest graph (about 80 bytes per vertex); when the device cannot
+ * hold one per team, fewer teams of the same size run. */
 int trav_batch_run(trav_batch *b, const trav_query *queries, int32_t n, float *device_ms);
 
 /* Time candidate shapes on these queries (each run `reps` times, best kept)

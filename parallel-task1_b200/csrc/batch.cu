@@ -219,7 +219,22 @@ int run_launch(trav_batch *b, int32_t n, const trav_batch_shape &s, float *ms)
     const int most = persistent_grid_size(2);
     if (most <= 0) return TRAV_ERR_CUDA;
     TRY(shape_ok(s, most));
-    const int teams = std::max(1, std::min(most / s.team_ctas, (int)n));
+    int teams = std::max(1, std::min(most / s.team_ctas, (int)n));
+    if (teams > b->teams_alloc) {
+        // every team needs scratch for the batch's largest graph: run fewer
+        // teams (each still of team_ctas CTAs) when the device cannot hold them
+        size_t free_b = 0, total_b = 0;
+        TRY_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const size_t have = (size_t)b->teams_alloc * b->team_bytes + free_b;
+        const size_t spare = (size_t)1 << 30;  // left for the caller
+        const size_t per = team_layout(b).total + sizeof(Ctl) + sizeof(TeamWs);
+        const size_t fit = have > spare ? (have - spare) / per : 0;
+        if (fit < 1) {
+            set_error("batch: not enough device memory for one team's scratch");
+            return TRAV_ERR_OOM;
+        }
+        teams = (int)std::min<size_t>((size_t)teams, fit);
+    }
     TRY(ensure_teams(b, teams));
     for (int t = 0; t < teams; t++) TRY_CUDA(cudaMemsetAsync(b->ctl + t, 0, offsetof(Ctl, dirs), b->st));
     BatchArgs a{};
