@@ -465,7 +465,7 @@ __device__ void write_back(const TravArgs &a)
 #define TRAV_KBATCH_BFS 4
 #endif
 #ifndef TRAV_KBATCH_SSSP
-#define TRAV_KBATCH_SSSP 2
+#define TRAV_KBATCH_SSSP 3
 #endif
 #ifndef TRAV_SSSP_MIN_BLOCKS
 #define TRAV_SSSP_MIN_BLOCKS 4
@@ -480,8 +480,10 @@ __device__ void write_back(const TravArgs &a)
 #define TRAV_FLUSH_ATTR __forceinline__
 #endif
 // Independent edges per lane per round of a relaxation loop.  More edges in
-// flight hide more latency but cost registers: SSSP's 64-register budget
-// (4 CTAs per SM) holds 2 without spilling, and 4 took 30% longer at s23.
+// flight hide more latency but cost registers.  With the atomics deferred
+// (SsspPush), SSSP's 64-register budget (4 CTAs per SM) holds 3 without
+// spilling; at s23 a batch of 128 queries ran 8% faster with 3 than with 2,
+// and 4 gained nothing more.  5 CTAs per SM (48 registers) spill and lose 50%.
 constexpr int kBatchBfs = TRAV_KBATCH_BFS, kBatchSssp = TRAV_KBATCH_SSSP;
 // Per-warp buffers: a push adds at most 32 entries to a buffer that held
 // fewer than its flush mark, so mark + 32 entries always fit.
@@ -497,6 +499,15 @@ struct WarpStage {
     int far[kWFar];
     int tu[32], trb[32], tpre[32];  // the current warp tile
     float tdu[32];
+};
+
+// Deferred SSSP relaxations of one warp (see SsspPush): fewer than 32 kept
+// between batches, plus up to 32 per edge of a lane's batch.
+constexpr int kWDefer = 32 + 32 * kBatchSssp;
+struct DeferStage {
+    int v[kWDefer];
+    float d[kWDefer];
+    unsigned cls[kWDefer];
 };
 
 struct CtaCounters {
@@ -522,7 +533,9 @@ struct Pusher {
     const TravArgs *a;
     const FrontierOut *o;
     WarpStage *s;
+    DeferStage *d;                   // the warp's deferred relaxations (SSSP expansions only)
     unsigned nq[2], nbig[2], nfar;
+    unsigned ndef;                   // entries staged in d
     unsigned big_total[2];
     unsigned long long mf, scanned;  // lane-partial sums
     int far_key;                     // lane-partial max
@@ -537,13 +550,16 @@ __device__ __forceinline__ int2 row_part(const TravArgs &a, int v, int part)
     return make_int2(rb, re);
 }
 
-__device__ __forceinline__ Pusher make_pusher(const TravArgs &a, const FrontierOut &o, WarpStage *s)
+__device__ __forceinline__ Pusher make_pusher(const TravArgs &a, const FrontierOut &o, WarpStage *s,
+                                              DeferStage *d = nullptr)
 {
     Pusher p;
     p.a = &a;
     p.o = &o;
     p.s = s;
+    p.d = d;
     p.nq[0] = p.nq[1] = p.nbig[0] = p.nbig[1] = p.nfar = 0;
+    p.ndef = 0;
     p.big_total[0] = p.big_total[1] = 0;
     p.mf = p.scanned = 0;
     p.far_key = 0;
@@ -750,6 +766,7 @@ __device__ void expand_frontier(const TravArgs &a, const int32_t *q, unsigned nq
         }
         __syncwarp();
     }
+    vis.finish(p);
 }
 
 // One vertex as a frontier of its own (row part [rb, re)): every CTA computes
@@ -778,6 +795,7 @@ struct BfsPush {
     int level_next;
 
     __device__ __forceinline__ float begin(int) const { return 0.0f; }
+    __device__ __forceinline__ void finish(Pusher &) const {}
 
     __device__ __forceinline__ void load_at(const int (&e)[kBatch], const bool (&ok)[kBatch], int (&v)[kBatch],
                                             float (&)[kBatch]) const
@@ -879,6 +897,14 @@ struct SsspPush {
         visit_loaded(du, v, w, ok, p);
     }
 
+    // An edge whose candidate beats the gathered distance is not relaxed at
+    // once: (v, candidate, row class) goes to the warp's DeferStage, and the
+    // atomicMins run 32 at a time (drain).  A batch then waits on its edge
+    // loads and its gathers only; the wait for an atomic's return -- which
+    // every batch used to pay, since almost every batch of 32 * kBatch edges
+    // has an improving lane -- comes once per 32 candidates.  The candidates
+    // are relaxed within the same phase, and the push decision reads only the
+    // atomic's return value, so the order of the atomics changes nothing.
     __device__ __forceinline__ void visit_loaded(const float (&du)[kBatch], const int (&v)[kBatch],
                                                  const float (&w)[kBatch], const bool (&ok)[kBatch], Pusher &p) const
     {
@@ -888,35 +914,65 @@ struct SsspPush {
         for (int j = 0; j < kBatch; j++) nd[j] = ok[j] ? __fadd_rn(du[j], w[j]) : 0.0f;  // one rounded add, as sssp.hpp:56
 #pragma unroll
         for (int j = 0; j < kBatch; j++) cur[j] = ok[j] ? ld_gather(&a->dist[v[j]]) : 0ull;
-        bool light[kBatch], heavy[kBatch], far[kBatch];
+        DeferStage *d = p.d;
 #pragma unroll
         for (int j = 0; j < kBatch; j++) {
-            light[j] = heavy[j] = far[j] = false;
-            if (ok[j] && nd[j] < dist_of(cur[j])) {
-                const unsigned cls = (unsigned)cur[j] & kClsMask;
-                const unsigned long long old =
-                    atomicMin(&a->dist[v[j]], pack_dist(nd[j], round << kClsBits | cls));
-                const float od = dist_of(old);
-                if (nd[j] < od) {
-                    const unsigned orr = (unsigned)old >> kClsBits;
-                    if (nd[j] < thr) {
-                        const bool seen_below = od < thr;
-                        light[j] = (cls & kClsLight) && !(seen_below && orr >= round);
-                        heavy[j] = (cls & kClsHeavy) && !(seen_below && orr >= h_start);
-                    } else {
-                        far[j] = !(orr >= f_start);  // od > nd >= thr
-                    }
+            const bool cand = ok[j] && nd[j] < dist_of(cur[j]);
+            const unsigned m = __ballot_sync(kFull, cand);
+            if (cand) {
+                const unsigned i = p.ndef + __popc(m & lanemask_lt());
+                d->v[i] = v[j];
+                d->d[i] = nd[j];
+                d->cls[i] = (unsigned)cur[j] & kClsMask;
+            }
+            p.ndef += __popc(m);
+        }
+        while (p.ndef >= 32) drain(p, 32);
+    }
+
+    // End of the warp's expansion: relax what is still staged.
+    __device__ __forceinline__ void finish(Pusher &p) const
+    {
+        if (p.ndef) drain(p, p.ndef);
+    }
+
+    // Relax the last n (<= 32) staged candidates, one per lane, and push the
+    // vertices they improved.  Warp-collective.
+    __device__ __forceinline__ void drain(Pusher &p, unsigned n) const
+    {
+        __syncwarp();
+        const DeferStage *d = p.d;
+        const unsigned base = p.ndef - n, lane = lane_id();
+        const bool ok = lane < n;
+        int v = 0;
+        float nd = 0.0f;
+        unsigned cls = 0;
+        if (ok) {
+            v = d->v[base + lane];
+            nd = d->d[base + lane];
+            cls = d->cls[base + lane];
+        }
+        __syncwarp();  // the entries are read before later batches overwrite them
+        p.ndef = base;
+        bool light = false, heavy = false, far = false;
+        if (ok) {
+            const unsigned long long old = atomicMin(&a->dist[v], pack_dist(nd, round << kClsBits | cls));
+            const float od = dist_of(old);
+            if (nd < od) {
+                const unsigned orr = (unsigned)old >> kClsBits;
+                if (nd < thr) {
+                    const bool seen_below = od < thr;
+                    light = (cls & kClsLight) && !(seen_below && orr >= round);
+                    heavy = (cls & kClsHeavy) && !(seen_below && orr >= h_start);
+                } else {
+                    far = !(orr >= f_start);  // od > nd >= thr
                 }
             }
         }
         const unsigned big_len = (unsigned)a->small_deg + 1u;  // any length that classifies as a long row
-#pragma unroll
-        for (int j = 0; j < kBatch; j++) {
-            const unsigned cls = (unsigned)cur[j];
-            push(p, 0, light[j], v[j], cls & kClsLightBig ? big_len : 1u);
-            push(p, 1, heavy[j], v[j], cls & kClsHeavyBig ? big_len : 1u);
-            push_far(p, far[j], v[j], far[j] ? 0x7fffffff - __float_as_int(nd[j]) : 0);
-        }
+        push(p, 0, light, v, cls & kClsLightBig ? big_len : 1u);
+        push(p, 1, heavy, v, cls & kClsHeavyBig ? big_len : 1u);
+        push_far(p, far, v, far ? 0x7fffffff - __float_as_int(nd) : 0);
     }
 };
 
@@ -1159,7 +1215,7 @@ __device__ __forceinline__ unsigned row_class(const TravArgs &a, int v)
            (nh > a.small_deg ? kClsHeavyBig : 0u);
 }
 
-__device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, int ph0)
+__device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, DeferStage *defer, int ph0)
 {
     SlotView &s_view = sh.view;
     PhaseLog lg;
@@ -1171,6 +1227,7 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, in
     const int gtid = team_tid(a), nth = team_threads(a);
     const unsigned gwarp = gtid >> 5, nwarps = nth >> 5;
     WarpStage *mys = &wst[threadIdx.x >> 5];
+    DeferStage *myd = &defer[threadIdx.x >> 5];
     const int lpart = a.nlight ? kPartLight : kPartWhole;
     const unsigned big_len = (unsigned)a.small_deg + 1u;  // any length that classifies as a long row
     int ph = ph0;
@@ -1249,7 +1306,7 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, in
                                   (fcur ? a.far1 : a.far0),
                                   (unsigned)far_len,
                                   &ctl->slot[ph % kSlots]};
-            Pusher p = make_pusher(a, out, mys);
+            Pusher p = make_pusher(a, out, mys, myd);
             const SsspPush vis{&a, thr, (unsigned)ph, h_start, f_start};
             if (lpart == kPartLight)
                 expand_frontier<kPartLight>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, p);
@@ -1283,7 +1340,7 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, in
                                   (fcur ? a.far1 : a.far0),
                                   (unsigned)far_len,
                                   &ctl->slot[ph % kSlots]};
-            Pusher p = make_pusher(a, out, mys);
+            Pusher p = make_pusher(a, out, mys, myd);
             h_start = (unsigned)ph;  // the next heavy list begins in this round
             const SsspPush vis{&a, thr, (unsigned)ph, h_start, f_start};
             expand_frontier<kPartHeavy>(a, (hcur ? a.hq1 : a.hq0), hq, (hcur ? a.hch1 : a.hch0), hch, vis, p);
@@ -1385,7 +1442,8 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, in
 __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) sssp_persistent(TravArgs a)
 {
     __shared__ QueryShared sh;
-    sssp_query(a, sh, 0);
+    __shared__ DeferStage defer[kWarps];
+    sssp_query(a, sh, defer, 0);
 }
 
 // ------------------------------------------------------------ batch kernel
@@ -1399,6 +1457,7 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) sssp_persistent(
 __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) batch_persistent(BatchArgs b)
 {
     __shared__ QueryShared sh;
+    __shared__ DeferStage defer[kWarps];  // used by the SSSP queries
     const int team = (int)blockIdx.x / b.team_ctas;
     const TeamWs w = b.teams[team];
     TravArgs t{};
@@ -1467,7 +1526,7 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) batch_persistent
             a.mean_w = q.mean_w;
             a.max_deg = q.max_deg;
             a.out_kind = 1;
-            ph = sssp_query(a, sh, ph);
+            ph = sssp_query(a, sh, defer, ph);
         }
         if (ph < 0) return;
     }
