@@ -365,14 +365,17 @@ def run_ours(a):
     assert np.array_equal(runs[primary]["di"].view(np.uint32), di_dev.cpu().numpy().view(np.uint32))
 
     # e2e through the public API with pinned host buffers: per step, the query descriptors (source ids inside)
-    # go H2D in the call and every level / distance array comes back D2H.  The step runs as four launches of a
-    # quarter of the queries; each quarter's results are copied on a second stream while the next quarter runs.
-    # Timed on the host clock.
+    # go H2D in the call and every level / distance array comes back D2H.  The step runs as four launches over
+    # 24/64, 20/64, 14/64 and 6/64 of the sources; each part's results are copied on a second stream while the
+    # next part runs.  The parts shrink so that each copy still ends within the next part's launch (the copy of
+    # a part takes about 0.4 of its compute time) and only the small last part's copy is left after the last
+    # launch.  Timed on the host clock.
     lv_host = torch.empty((n, V), dtype=torch.int32).pin_memory()
     di_host = torch.empty((n, V), dtype=torch.float32).pin_memory()
     cs = torch.cuda.Stream()
-    parts = 4
-    cut = [round(i * n / parts) for i in range(parts + 1)]
+    frac = [0, 24, 44, 58, 64]
+    cut = sorted(set([0] + [round(n * f / 64) for f in frac[1:]])) if n else [0]
+    parts = len(cut) - 1
     chunks = [queries[primary][cut[i]:cut[i + 1]] + queries[primary][n + cut[i]:n + cut[i + 1]] for i in range(parts)]
 
     def e2e_step():
