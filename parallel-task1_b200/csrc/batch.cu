@@ -163,6 +163,7 @@ int build_queries(trav_batch *b, const trav_query *qs, int32_t n, std::vector<Ba
         d.out_w = g->g.out_w;
         d.in_off = g->g.in_off;
         d.in_adj = g->g.in_adj;
+        d.in_w = g->g.in_w;
         d.new_of_old = g->g.new_of_old;
         d.V = g->g.V;
         d.E = g->g.E;

@@ -144,7 +144,7 @@ __global__ void relabel_kernel(int32_t V, const int32_t *__restrict__ old_of_new
 __global__ void edge_keys_kernel(int64_t E, int lv, const int32_t *__restrict__ src, const int32_t *__restrict__ dst,
                                  const int32_t *__restrict__ new_of_old, const float *__restrict__ w,
                                  unsigned long long *__restrict__ out_keys, unsigned long long *__restrict__ in_keys,
-                                 int32_t *__restrict__ out_dst)
+                                 int32_t *__restrict__ out_dst, float *__restrict__ in_wt)
 {
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
         unsigned long long s = (unsigned)new_of_old[src[e]], t = (unsigned)new_of_old[dst[e]];
@@ -153,6 +153,7 @@ __global__ void edge_keys_kernel(int64_t E, int lv, const int32_t *__restrict__ 
         out_keys[e] = (s << 32) | __float_as_uint(wt);
         in_keys[e] = (t << lv) | s;
         out_dst[e] = (int32_t)t;
+        in_wt[e] = wt;
     }
 }
 
@@ -289,6 +290,7 @@ void free_graph(DevGraph *g)
     cudaFree(g->out_w);
     cudaFree(g->in_off);
     cudaFree(g->in_adj);
+    cudaFree(g->in_w);
     cudaFree(g->new_of_old);
     cudaFree(g->old_of_new);
     *g = DevGraph{};
@@ -305,7 +307,7 @@ int build_graph_device(int32_t V, int64_t E, const int32_t *d_src, const int32_t
 
     DBuf<int32_t> out_deg, in_deg, ids, deg_sorted, out_deg_new, in_deg_new;
     DBuf<int32_t> out_off, in_off, new_of_old, old_of_new, out_adj, in_adj;
-    DBuf<float> out_w;
+    DBuf<float> out_w, in_w, iwt;
     DBuf<int32_t> dv;
     DBuf<unsigned long long> okeys, ikeys, skeys;
     TRY_CUDA(out_deg.alloc(V));
@@ -321,6 +323,7 @@ int build_graph_device(int32_t V, int64_t E, const int32_t *d_src, const int32_t
     TRY_CUDA(out_adj.alloc(E));
     TRY_CUDA(in_adj.alloc(E));
     TRY_CUDA(out_w.alloc(E));
+    TRY_CUDA(in_w.alloc(E));
 
     TRY_CUDA(cudaMemsetAsync(out_deg.p, 0, sizeof(int32_t) * (size_t)V, st));
     TRY_CUDA(cudaMemsetAsync(in_deg.p, 0, sizeof(int32_t) * (size_t)V, st));
@@ -338,8 +341,9 @@ int build_graph_device(int32_t V, int64_t E, const int32_t *d_src, const int32_t
         TRY_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb3, (unsigned long long *)nullptr,
                                                  (unsigned long long *)nullptr, (int32_t *)nullptr, (int32_t *)nullptr,
                                                  (int)E, 0, 32 + lv, st));
-        TRY_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tb4, (unsigned long long *)nullptr,
-                                                (unsigned long long *)nullptr, (int)E, 0, 2 * lv, st));
+        TRY_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb4, (unsigned long long *)nullptr,
+                                                 (unsigned long long *)nullptr, (float *)nullptr, (float *)nullptr,
+                                                 (int)E, 0, 2 * lv, st));
     }
     size_t tmax = tb;
     if (tb2 > tmax) tmax = tb2;
@@ -360,13 +364,16 @@ int build_graph_device(int32_t V, int64_t E, const int32_t *d_src, const int32_t
         TRY_CUDA(ikeys.alloc(E));
         TRY_CUDA(skeys.alloc(E));
         TRY_CUDA(dv.alloc(E));
-        edge_keys_kernel<<<grid_for(E), 256, 0, st>>>(E, lv, d_src, d_dst, new_of_old.p, d_w, okeys.p, ikeys.p, dv.p);
+        TRY_CUDA(iwt.alloc(E));
+        edge_keys_kernel<<<grid_for(E), 256, 0, st>>>(E, lv, d_src, d_dst, new_of_old.p, d_w, okeys.p, ikeys.p, dv.p,
+                                                      iwt.p);
         TRY_CUDA(cudaGetLastError());
         // Out rows by (new source, weight); stable, so equal weights keep
         // their edge-list order.
         TRY_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, tb3, okeys.p, skeys.p, dv.p, out_adj.p, (int)E, 0, 32 + lv, st));
         low_word_float_kernel<<<grid_for(E), 256, 0, st>>>(E, skeys.p, out_w.p);
-        TRY_CUDA(cub::DeviceRadixSort::SortKeys(temp.p, tb4, ikeys.p, skeys.p, (int)E, 0, 2 * lv, st));
+        // In rows by (new target, new source), each in-edge with its weight.
+        TRY_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, tb4, ikeys.p, skeys.p, iwt.p, in_w.p, (int)E, 0, 2 * lv, st));
         low_bits_kernel<<<grid_for(E), 256, 0, st>>>(E, mask, skeys.p, in_adj.p);
         TRY_CUDA(cudaGetLastError());
     }
@@ -394,6 +401,7 @@ int build_graph_device(int32_t V, int64_t E, const int32_t *d_src, const int32_t
     out->out_w = out_w.release();
     out->in_off = in_off.release();
     out->in_adj = in_adj.release();
+    out->in_w = in_w.release();
     out->new_of_old = new_of_old.release();
     out->old_of_new = old_of_new.release();
     return TRAV_OK;

@@ -94,6 +94,7 @@ struct DevGraph {
     float *out_w = nullptr;       // E
     int32_t *in_off = nullptr;    // V+1
     int32_t *in_adj = nullptr;    // E
+    float *in_w = nullptr;        // E: weight of each in-edge (the SSSP pull rounds)
     int32_t *new_of_old = nullptr;  // V
     int32_t *old_of_new = nullptr;  // V
 };
@@ -131,6 +132,7 @@ struct TravArgs {
     const float *__restrict__ out_w;
     const int32_t *__restrict__ in_off;
     const int32_t *__restrict__ in_adj;
+    const float *__restrict__ in_w;   // in-edge weights; nullptr = no SSSP pull rounds
     const int32_t *__restrict__ new_of_old;
     int32_t V;
     int32_t W;        // bitmap words
@@ -178,7 +180,7 @@ struct TravArgs {
 // One query of a batch launch (device descriptor, built by the host).
 struct BatchQuery {
     const int32_t *out_off, *out_adj, *in_off, *in_adj, *new_of_old;
-    const float *out_w;
+    const float *out_w, *in_w;
     const int32_t *nlight;  // SSSP light-prefix lengths for delta; nullptr = Bellman-Ford
     const float *mlp;       // schedule network; nullptr = plain schedule
     void *out;              // results in original ids: int32 levels (BFS) or float distances (SSSP)

@@ -491,7 +491,13 @@ constexpr int kWQFlush = 128, kWQ = kWQFlush + 32;
 constexpr int kWBigFlush = 64, kWBig = kWBigFlush + 32;
 constexpr int kWFarFlush = 128, kWFar = kWFarFlush + 32;
 
-constexpr int kPartWhole = 0, kPartLight = 1, kPartHeavy = 2;
+constexpr int kPartWhole = 0, kPartLight = 1, kPartHeavy = 2, kPartIn = 3;  // kPartIn: the in-row (CSC)
+// An SSSP heavy round considers pulling when its heavy list may hold more than
+// 1/kPullCheck of the graph's edges.
+#ifndef TRAV_PULL_CHECK
+#define TRAV_PULL_CHECK 8.0
+#endif
+constexpr double kPullCheck = TRAV_PULL_CHECK;
 
 struct WarpStage {
     int q[2][kWQ];
@@ -544,6 +550,7 @@ struct Pusher {
 // Row part [begin, end) of vertex v.
 __device__ __forceinline__ int2 row_part(const TravArgs &a, int v, int part)
 {
+    if (part == kPartIn) return make_int2(__ldg(&a.in_off[v]), __ldg(&a.in_off[v + 1]));
     int rb = __ldg(&a.out_off[v]), re = __ldg(&a.out_off[v + 1]);
     if (part == kPartLight) re = rb + __ldg(&a.nlight[v]);
     else if (part == kPartHeavy) rb += __ldg(&a.nlight[v]);
@@ -868,7 +875,21 @@ __device__ __forceinline__ unsigned long long pack_dist(float d, unsigned low)
 // Among the threads that lower one vertex in a round, exactly the first one
 // sees an old word from an earlier round (distances only fall, so a vertex
 // below the bound stays below it).
-struct SsspPush {
+__device__ __forceinline__ unsigned row_class(const TravArgs &a, int v)
+{
+    const int deg = __ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v]);
+    const int nl = a.nlight ? __ldg(&a.nlight[v]) : deg, nh = deg - nl;
+    return (nl > 0 ? kClsLight : 0u) | (nl > a.small_deg ? kClsLightBig : 0u) | (nh > 0 ? kClsHeavy : 0u) |
+           (nh > a.small_deg ? kClsHeavyBig : 0u);
+}
+
+// kPull = false relaxes out-rows (push): the row's owner is the source of
+// every candidate.  kPull = true scans the in-rows of unsettled vertices
+// (pull rounds): the row's owner is the target, and each in-edge u -> owner
+// gives the candidate fl(d(u) + w).  Both feed the same deferred atomics and
+// push decisions; a pull candidate is just a relaxation of the edge u -> owner.
+template <bool kPull>
+struct SsspVisit {
     static constexpr int kBatch = kBatchSssp;
     const TravArgs *a;
     float thr;               // bucket upper bound (exclusive)
@@ -888,13 +909,39 @@ struct SsspPush {
         }
     }
 
-    __device__ __forceinline__ void visit_batch(const int (&)[kBatch], const float (&du)[kBatch],
+    __device__ __forceinline__ void visit_batch(const int (&us)[kBatch], const float (&du)[kBatch],
                                                 const int (&e)[kBatch], const bool (&ok)[kBatch], Pusher &p) const
     {
         int v[kBatch];
         float w[kBatch];
-        load_at(e, ok, v, w);
-        visit_loaded(du, v, w, ok, p);
+        if constexpr (kPull) {
+            // in-neighbours and weights; the candidate's target is the row's owner us[j], whose distance is du[j]
+#pragma unroll
+            for (int j = 0; j < kBatch; j++) {
+                v[j] = ok[j] ? ld_stream(&a->in_adj[e[j]]) : 0;
+                w[j] = ok[j] ? ld_stream(&a->in_w[e[j]]) : 0.0f;
+            }
+            float nd[kBatch];
+#pragma unroll
+            for (int j = 0; j < kBatch; j++) nd[j] = ok[j] ? dist_of(ld_gather(&a->dist[v[j]])) : 0.0f;
+            DeferStage *d = p.d;
+#pragma unroll
+            for (int j = 0; j < kBatch; j++) {
+                nd[j] = __fadd_rn(nd[j], w[j]);  // one rounded add, as sssp.hpp:56
+                const bool cand = ok[j] && nd[j] < du[j];
+                const unsigned m = __ballot_sync(kFull, cand);
+                if (cand) {
+                    const unsigned i = p.ndef + __popc(m & lanemask_lt());
+                    d->v[i] = us[j];
+                    d->d[i] = nd[j];
+                }
+                p.ndef += __popc(m);
+            }
+            while (p.ndef >= 32) drain(p, 32);
+        } else {
+            load_at(e, ok, v, w);
+            visit_loaded(du, v, w, ok, p);
+        }
     }
 
     // An edge whose candidate beats the gathered distance is not relaxed at
@@ -950,9 +997,12 @@ struct SsspPush {
         if (ok) {
             v = d->v[base + lane];
             nd = d->d[base + lane];
-            cls = d->cls[base + lane];
+            if constexpr (!kPull) cls = d->cls[base + lane];
         }
         __syncwarp();  // the entries are read before later batches overwrite them
+        if constexpr (kPull) {
+            if (ok) cls = row_class(*a, v);  // the owner's flags (a pull stages no gathered word of it)
+        }
         p.ndef = base;
         bool light = false, heavy = false, far = false;
         if (ok) {
@@ -975,6 +1025,9 @@ struct SsspPush {
         push_far(p, far, v, far ? 0x7fffffff - __float_as_int(nd) : 0);
     }
 };
+
+using SsspPush = SsspVisit<false>;
+using SsspPull = SsspVisit<true>;
 
 __device__ __forceinline__ void init_counters(CtaCounters &cc)
 {
@@ -1207,14 +1260,6 @@ __global__ void __launch_bounds__(kBlock, TRAV_BFS_MIN_BLOCKS) bfs_persistent(Tr
 // lowering a distance, so it stamps each vertex it pushes with its own round
 // (an atomicMax that keeps the distance: nothing lowers distances in that
 // phase).
-__device__ __forceinline__ unsigned row_class(const TravArgs &a, int v)
-{
-    const int deg = __ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v]);
-    const int nl = a.nlight ? __ldg(&a.nlight[v]) : deg, nh = deg - nl;
-    return (nl > 0 ? kClsLight : 0u) | (nl > a.small_deg ? kClsLightBig : 0u) | (nh > 0 ? kClsHeavy : 0u) |
-           (nh > a.small_deg ? kClsHeavyBig : 0u);
-}
-
 __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, DeferStage *defer, int ph0)
 {
     SlotView &s_view = sh.view;
@@ -1238,6 +1283,7 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
     unsigned long long far_len = 0;
     int min_far = (int)kFltMaxBits;
     float thr = a.delta > 0.0f ? a.delta : INFINITY;
+    float lo = 0.0f;                        // lower bound of the current bucket
     int cur = 0, hcur = 0, fcur = 0;
 
     unsigned h_start = 1, f_start = 1;      // rounds the heavy list / far pile began in
@@ -1330,7 +1376,40 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
             cur ^= 1;
             steps++;
         } else if (hq + hch > 0) {
-            // heavy round: heavy list (hcur) -> frontier (cur, empty) + next heavy list (hcur^1)
+            // heavy round: heavy list (hcur) -> frontier (cur, empty) + next heavy list (hcur^1).
+            // Direction: when the heavy list's heavy parts may hold more than 1/kPullCheck of the edges, a check
+            // phase first lists the vertices that a heavy edge could still improve, in the idle frontier buffer,
+            // and counts their in-edges.  If they are fewer than half the heavy edges, the round pulls: it scans
+            // those in-rows, and every in-edge u -> v relaxes v from u's distance, instead of pushing the heavy
+            // list's out-rows.  The heavy list lies at or above the bucket's lower bound lo and a heavy edge
+            // weighs at least delta, so a heavy candidate is at least fl(lo + delta): a vertex at or below that
+            // cannot improve, and every other vertex is in the list.
+            bool pull = false;
+            unsigned pq = 0, pch = 0;
+            const double heavy_est = (double)hch * a.item + (double)hq * (0.5 * a.small_deg + 1.0);
+            if (a.in_w && heavy_est * kPullCheck > (double)a.E) {
+                const float reach = __fadd_rn(lo, a.delta);
+                clear_ahead(a, ph);
+                const FrontierOut lout{{(cur ? a.q0 : a.q1), nullptr}, {(cur ? a.chunks0 : a.chunks1), nullptr},
+                                       {0u, 0u}, {0u, 0u}, {kPartIn, kPartIn}, nullptr, 0u, &ctl->slot[ph % kSlots]};
+                Pusher lp = make_pusher(a, lout, mys);
+                for (unsigned base = gwarp * 32; base < (unsigned)a.V; base += nwarps * 32) {
+                    const int v = (int)(base + lane_id());
+                    unsigned len = 0;
+                    if (v < a.V && dist_of(__ldcg(&a.dist[v])) > reach)
+                        len = (unsigned)(__ldg(&a.in_off[v + 1]) - __ldg(&a.in_off[v]));
+                    lp.mf += len;  // a lane's share stays below E < 2^31
+                    push(lp, 0, len > 0, v, len);
+                }
+                finish_phase(lp, cc);
+                if (!grid_sync(a, ph, &s_view)) return -1;
+                log_phase(ctl, lg, 6, s_view.q_add + s_view.big_add);
+                pq = s_view.q_add;
+                pch = s_view.chunk_add;
+                pull = 2.0 * (double)s_view.mf < heavy_est;
+                ph++;
+                steps++;
+            }
             clear_ahead(a, ph);
             const FrontierOut out{{(cur ? a.q1 : a.q0), (hcur ? a.hq0 : a.hq1)},
                                   {(cur ? a.chunks1 : a.chunks0), (hcur ? a.hch0 : a.hch1)},
@@ -1342,12 +1421,17 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
                                   &ctl->slot[ph % kSlots]};
             Pusher p = make_pusher(a, out, mys, myd);
             h_start = (unsigned)ph;  // the next heavy list begins in this round
-            const SsspPush vis{&a, thr, (unsigned)ph, h_start, f_start};
-            expand_frontier<kPartHeavy>(a, (hcur ? a.hq1 : a.hq0), hq, (hcur ? a.hch1 : a.hch0), hch, vis, p);
+            if (pull) {
+                const SsspPull vis{&a, thr, (unsigned)ph, h_start, f_start};
+                expand_frontier<kPartIn>(a, (cur ? a.q0 : a.q1), pq, (cur ? a.chunks0 : a.chunks1), pch, vis, p);
+            } else {
+                const SsspPush vis{&a, thr, (unsigned)ph, h_start, f_start};
+                expand_frontier<kPartHeavy>(a, (hcur ? a.hq1 : a.hq0), hq, (hcur ? a.hch1 : a.hch0), hch, vis, p);
+            }
             finish_phase(p, cc);
             if (!grid_sync(a, ph, &s_view)) return -1;
             lg.scanned += s_view.scanned;
-            log_phase(ctl, lg, 5, hq + hbig);
+            log_phase(ctl, lg, pull ? 7 : 5, hq + hbig);
             const SlotView s0 = s_view;
             ph++;
             nq = s0.q_add;
@@ -1378,6 +1462,7 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
             __syncthreads();
             const float told = thr;
             thr = s_delta;  // the new bound, computed once above (same inputs in every CTA)
+            lo = fmaxf(told, __int_as_float(min_far));
             const int32_t *fp = fcur ? a.far1 : a.far0;
             clear_ahead(a, ph);
             // the (empty) frontier and heavy list receive the entries of the new bucket
@@ -1482,6 +1567,7 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) batch_persistent
         a.out_w = q.out_w;
         a.in_off = q.in_off;
         a.in_adj = q.in_adj;
+        a.in_w = q.in_w;
         a.new_of_old = q.new_of_old;
         a.V = q.V;
         a.W = (q.V + 31) / 32;
@@ -1810,6 +1896,7 @@ static TravArgs make_args(const DevGraph &g, Workspace *ws)
     a.out_w = g.out_w;
     a.in_off = g.in_off;
     a.in_adj = g.in_adj;
+    a.in_w = g.in_w;
     a.new_of_old = g.new_of_old;
     a.V = g.V;
     a.W = (g.V + 31) / 32;
