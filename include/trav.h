@@ -112,6 +112,11 @@ int trav_graph_info(const trav_graph *g, int32_t *vertices, int64_t *edges, int3
 int trav_graph_export(const trav_graph *g, int32_t *new_of_old, int32_t *old_of_new, int32_t *out_off,
                       int32_t *out_adj, float *out_w, int32_t *in_off, int32_t *in_adj);
 
+/* Copy the weight of every in-edge (in_w[E], the order of in_adj) to a host
+ * array.  The reference keeps no transposed weights; the SSSP pull rounds
+ * read them. */
+int trav_graph_export_in_w(const trav_graph *g, float *in_w);
+
 /* ----------------------------------------------------------------- queries */
 
 /* BFS levels from each of n sources: levels[q*V + v].  Replaces

@@ -373,6 +373,15 @@ int trav_graph_export(const trav_graph *g, int32_t *new_of_old, int32_t *old_of_
     return TRAV_OK;
 }
 
+int trav_graph_export_in_w(const trav_graph *g, float *in_w)
+{
+    if (!g) return bad("graph handle is NULL");
+    if (!in_w && g->g.E > 0) return bad("in_w must not be NULL");
+    cudaSetDevice(g->device);
+    if (g->g.E > 0) TRY_CUDA(cudaMemcpy(in_w, g->g.in_w, 4 * (size_t)g->g.E, cudaMemcpyDeviceToHost));
+    return TRAV_OK;
+}
+
 int trav_bfs(trav_graph *g, const int32_t *sources, int32_t n, const trav_bfs_opts *opts, int32_t *levels,
              int32_t mem)
 {

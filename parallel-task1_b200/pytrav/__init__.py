@@ -44,6 +44,7 @@ FLT_MAX = np.float32(np.finfo(np.float32).max)
 # Every symbol include/trav.h declares (checked by the CPU test suite).
 EXPORTS = [
     "trav_graph_from_edges", "trav_graph_rmat", "trav_graph_free", "trav_graph_info", "trav_graph_export",
+    "trav_graph_export_in_w",
     "trav_bfs", "trav_sssp", "trav_last_stats", "trav_last_bfs_trace", "trav_init_distances_f32",
     "trav_bellman_ford_el_f32", "trav_bfs_el", "trav_el_file_read", "trav_el_file_write", "trav_mlp_set",
     "trav_mlp_param_count", "trav_last_error", "trav_version", "trav_last_batch_ms", "trav_graph_set_stream",
@@ -103,6 +104,7 @@ def lib():
         L.trav_graph_free.argtypes = [vp]
         L.trav_graph_info.argtypes = [vp, C.POINTER(i32), C.POINTER(i64), C.POINTER(i32)]
         L.trav_graph_export.argtypes = [vp] * 8
+        L.trav_graph_export_in_w.argtypes = [vp, vp]
         L.trav_bfs.argtypes = [vp, vp, i32, C.POINTER(BfsOpts), vp, i32]
         L.trav_sssp.argtypes = [vp, vp, i32, C.POINTER(SsspOpts), vp, i32]
         L.trav_last_stats.argtypes = [vp, C.POINTER(QueryStats)]
@@ -334,6 +336,12 @@ class Graph:
         _check(lib().trav_graph_export(self._h, *(x.ctypes.data for x in (n2o, o2n, oo, oa, ow, io, ia))))
         return dict(new_of_old=n2o, old_of_new=o2n, out_off=oo, out_adj=oa[:E], out_w=ow[:E], in_off=io,
                     in_adj=ia[:E])
+
+    def export_in_w(self):
+        """Weight of every in-edge, in the order of the exported in_adj."""
+        iw = np.empty(max(self.E, 1), np.float32)
+        _check(lib().trav_graph_export_in_w(self._h, iw.ctypes.data))
+        return iw[: self.E]
 
 
 def mlp_param_count(kind: int) -> int:

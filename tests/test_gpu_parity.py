@@ -57,6 +57,25 @@ def test_device_layout_equals_oracle_layout(torch):
         assert g.max_out_degree == int(np.bincount(s, minlength=V).max())
 
 
+def test_device_in_edge_weights_follow_the_in_rows(torch):
+    # The CSC is one stable sort of the edges by (new target, new source), so its weights are the edge-list
+    # weights (-0.0 read as +0.0) in that order; the layout's in_adj pins the order itself.
+    for scale, avg, seed in [(6, 4, 1), (10, 8, 2), (13, 16, 5)]:
+        s, d, w = O.rmat(scale, avg, seed=seed)
+        w = w.copy()
+        w[::7] = -0.0
+        V = 1 << scale
+        g = T.Graph.from_edges(V, s, d, w)
+        want = O.device_layout(V, s, d, w)
+        n2o = want["new_of_old"]
+        ns, nd = n2o[s], n2o[d]
+        order = np.lexsort((ns, nd))
+        assert np.array_equal(ns[order], want["in_adj"])
+        w0 = np.where(w == 0.0, np.float32(0.0), w).astype(np.float32)
+        assert np.array_equal(bits(g.export_in_w()), bits(w0[order]))
+        g.free()
+
+
 def test_golden_cases_bfs_levels(golden, torch):
     meta, arrays = golden
     for name, c in meta["cases"].items():
