@@ -5,7 +5,7 @@ self-loop drop), a/b/c/d = 57/19/19/5, fp32 weights rand_r/RAND_MAX, seed 1, sel
 sources of nonzero out-degree.  One step = BFS (Beamer alpha 15 / beta 18) from each of the 64 sources plus
 SSSP (delta-stepping, delta 0.1) from each of them, the 128 queries run as one batched persistent launch
 (teams of CTAs, one query each at a time; shape autotuned outside the timed region).  TEPS = edges in the
-graph / traversal time (the reference's convention), summed over traversals.  The graph (3.3 GB of CSR, CSC
+graph / traversal time (the reference's convention), summed over traversals.  The graph (4.4 GB of CSR, CSC
 and in-edge weights) is larger than the 126 MB L2, so no flush runs between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--scale S] [--ef F]
