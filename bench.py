@@ -72,6 +72,13 @@ def pick_sources(deg, n, seed):
     return np.sort(rng.choice(cand, size=min(n, len(cand)), replace=False)).astype(np.int32)
 
 
+def e2e_cuts(n: int):
+    """Source boundaries of the e2e parts: 24/64, 20/64, 14/64 and 6/64 of n sources (fewer parts when n is
+    small), so that each part's result copy ends inside the next part's launch."""
+    frac = [24, 44, 58, 64]
+    return sorted(set([0] + [round(n * f / 64) for f in frac])) if n else [0]
+
+
 def rank_sources(deg, n, seed, rank):
     """Replica r of a weak-scaling run traverses its own seeded source set."""
     return pick_sources(deg, n, seed + rank)
@@ -373,8 +380,7 @@ def run_ours(a):
     lv_host = torch.empty((n, V), dtype=torch.int32).pin_memory()
     di_host = torch.empty((n, V), dtype=torch.float32).pin_memory()
     cs = torch.cuda.Stream()
-    frac = [0, 24, 44, 58, 64]
-    cut = sorted(set([0] + [round(n * f / 64) for f in frac[1:]])) if n else [0]
+    cut = e2e_cuts(n)
     parts = len(cut) - 1
     chunks = [queries[primary][cut[i]:cut[i + 1]] + queries[primary][n + cut[i]:n + cut[i + 1]] for i in range(parts)]
 
