@@ -359,7 +359,7 @@ int trav_graph_export(const trav_graph *g, int32_t *new_of_old, int32_t *old_of_
                       int32_t *out_adj, float *out_w, int32_t *in_off, int32_t *in_adj)
 {
     if (!g) return bad("graph handle is NULL");
-    cudaSetDevice(g->device);
+    TRY_CUDA(cudaSetDevice(g->device));
     const size_t V = (size_t)g->g.V, E = (size_t)g->g.E;
     if (new_of_old) TRY_CUDA(cudaMemcpy(new_of_old, g->g.new_of_old, 4 * V, cudaMemcpyDeviceToHost));
     if (old_of_new) TRY_CUDA(cudaMemcpy(old_of_new, g->g.old_of_new, 4 * V, cudaMemcpyDeviceToHost));
@@ -377,7 +377,7 @@ int trav_graph_export_in_w(const trav_graph *g, float *in_w)
 {
     if (!g) return bad("graph handle is NULL");
     if (!in_w && g->g.E > 0) return bad("in_w must not be NULL");
-    cudaSetDevice(g->device);
+    TRY_CUDA(cudaSetDevice(g->device));
     if (g->g.E > 0) TRY_CUDA(cudaMemcpy(in_w, g->g.in_w, 4 * (size_t)g->g.E, cudaMemcpyDeviceToHost));
     return TRAV_OK;
 }
