@@ -61,8 +61,37 @@ def dist_env():
 
 
 def workload_name(a):
+    """The workload both arms solve: the graph, the sources and the two queries per source.  How each arm
+    computes them (delta-stepping or Bellman-Ford; Beamer's switch or a level-synchronous top-down sweep) is
+    in the line's `implementation`; the distances and reachability are the same bits."""
     return (f"RMAT s{a.scale} ef{a.ef} a/b/c/d 57/19/19/5 seed {a.seed} loops dropped; {a.sources} sources; "
-            f"BFS Beamer a15/b18 + SSSP delta-stepping delta {a.delta}")
+            f"BFS + SSSP (delta {a.delta}) from each source")
+
+
+def bench_config(a, V, E, world):
+    """config of the JSON line; identical keys and values in both arms for the same arguments."""
+    return {"workload": workload_name(a), "scale": a.scale, "edge_factor": a.ef, "vertices": V, "edges": E,
+            "sources": a.sources, "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"}
+
+
+def host_cpu():
+    """CPU model, physical cores and logical CPUs of this host."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        import psutil
+
+        phys = psutil.cpu_count(logical=False)
+    except Exception:
+        phys = None
+    return {"cpu_model": model, "physical_cores": phys, "logical_cpus": os.cpu_count()}
 
 
 def pick_sources(deg, n, seed):
@@ -205,20 +234,25 @@ class CpuReference:
         self.gcsr = O.RefGraph.csr(V, off, adj, wt)
         self.next = 0
 
-    def sample(self, seconds):
-        """GTEPS of the GPU step's mix (one BFS + one SSSP per source) over about `seconds` of work."""
+    def sample(self, seconds, check=None):
+        """GTEPS of the GPU step's mix (one BFS + one SSSP per source) over about `seconds` of work.  With
+        `check`, check(source_index, reached, dist) is called after each source's two calls, outside their
+        timing brackets, with the reference's own results."""
         O = self.O
         t_sssp, t_bfs = [], []
         start = time.perf_counter()
         while not t_sssp or (time.perf_counter() - start) < seconds:
-            src = int(self.sources[self.next % len(self.sources)])
+            k = self.next % len(self.sources)
+            src = int(self.sources[k])
             self.next += 1
             t0 = O.ref().ref_wtime()
-            self.gcsr.parallel_bfs(src, threads=self.cores)
+            reached = self.gcsr.parallel_bfs(src, threads=self.cores)
             t_bfs.append(O.ref().ref_wtime() - t0)
             t0 = O.ref().ref_wtime()
-            self.gel.bellman_ford(src, threads=self.cores)
+            dist = self.gel.bellman_ford(src, threads=self.cores)
             t_sssp.append(O.ref().ref_wtime() - t0)
+            if check is not None:
+                check(k, reached, dist)
         per_source = statistics.mean(t_bfs) + statistics.mean(t_sssp)
         desc = (f"{len(t_bfs)} cpu_parallel_bfs + {len(t_sssp)} cpu_bellman_ford calls of the reference "
                 f"(oracle/_ref) on the same graph and sources with {self.cores} threads; GTEPS = 2E / (mean BFS + "
@@ -230,11 +264,26 @@ class CpuReference:
         self.gcsr.free()
 
 
-def cpu_reference_run(a, seconds):
+def cpu_reference_run(a, seconds, levels=None, dist=None):
+    """The CPU baseline leg: the reference's own path timed on a bounded sample.  With the GPU step's results
+    (levels[k], dist[k] of source k, original ids), every sampled source's reference results are compared with
+    them bit for bit: distances exactly, reachability as level >= 0; the returned parity record says how many
+    sources were compared and whether all were equal."""
     ref = CpuReference(a)
+    parity = {"sources": 0, "equal": True, "compared": "cpu_bellman_ford distance bits and cpu_parallel_bfs "
+                                                      "reachability of the same sources against the GPU step"}
+
+    def check(k, reached, d):
+        if levels is None:
+            return
+        same = (np.array_equal(d.view(np.uint32), dist[k].view(np.uint32))
+                and np.array_equal(reached.astype(bool), levels[k] >= 0))
+        parity["sources"] += 1
+        parity["equal"] = parity["equal"] and bool(same)
+
     try:
-        v, desc = ref.sample(seconds)
-        return v, desc, ref.cores, ref.E
+        v, desc = ref.sample(seconds, check=check if levels is not None else None)
+        return v, desc, ref.cores, ref.E, (parity if levels is not None else None)
     finally:
         ref.free()
 
@@ -257,10 +306,13 @@ def run_reference(a):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": 2 * E / value / 1e6, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded RMAT, generated here)",
-        "config": {"workload": workload_name(a), "scale": a.scale, "edge_factor": a.ef, "edges": E,
-                   "sources": a.sources},
-        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": cores, "kind": "reference", "sample": desc},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded RMAT generated here)",
+        "config": bench_config(a, 1 << a.scale, E, a.gpus),
+        "implementation": ("the reference's own CPU path (oracle/_ref, compiled from its sources): "
+                           "cpu_parallel_bfs (level-synchronous top-down, bool reachability) and cpu_bellman_ford "
+                           "(edge-list sweeps to the fixpoint) per source, all host threads"),
+        "cpu_baseline": dict({"value": value, "unit": "GTEPS", "cores": cores, "kind": "reference",
+                              "sample": desc}, **host_cpu()),
         "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -427,10 +479,11 @@ def run_ours(a):
             "warmup": a.warmup, "ms_per_step": runs[primary]["ms"] / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded RMAT generated on the device)",
-            "config": {"workload": workload_name(a), "scale": a.scale, "edge_factor": a.ef, "vertices": V,
-                       "edges": E, "sources": n, "schedule": names[primary], "l2": "inputs larger than L2 (no flush)",
-                       "execution": "each step's 2n queries in one batched persistent launch (autotuned teams)",
-                       "parallelism": f"replicas x{world}"},
+            "config": bench_config(a, V, E, world),
+            "implementation": (f"BFS direction-optimising (Beamer alpha 15 / beta 18 or the learned switch) and "
+                               f"SSSP delta-stepping (delta {a.delta}, light/heavy edges, pull rounds); each step's "
+                               f"2n queries in one batched persistent launch (autotuned teams)"),
+            "schedule": names[primary],
             "schedules": per,
             "sequential_launches": {"gteps": job_gteps(2 * n, E, 1, seq_ms / 1e3), "ms_per_step": seq_ms,
                                     "note": "the same step as one persistent launch per query, primary schedule"},
@@ -451,12 +504,14 @@ def run_ours(a):
             line["batched"] = batched_workload(a.seed)
         if not a.no_cpu_baseline and world == 1:
             try:
-                v, desc, cores, _ = cpu_reference_run(a, a.cpu_sample_s)
-                line["cpu_baseline"] = {"value": v, "unit": "GTEPS", "cores": cores, "kind": "reference",
-                                        "sample": desc}
+                v, desc, cores, _, parity = cpu_reference_run(a, a.cpu_sample_s, levels=runs[primary]["lv"],
+                                                              dist=runs[primary]["di"])
+                line["cpu_baseline"] = dict({"value": v, "unit": "GTEPS", "cores": cores, "kind": "reference",
+                                             "sample": desc}, **host_cpu())
+                line["parity"] = parity
             except Exception as ex:  # the baseline is reported, never required for the GPU number
-                line["cpu_baseline"] = {"value": None, "unit": "GTEPS", "cores": os.cpu_count(),
-                                        "kind": "reference", "sample": f"not run: {ex}"}
+                line["cpu_baseline"] = dict({"value": None, "unit": "GTEPS", "cores": os.cpu_count(),
+                                             "kind": "reference", "sample": f"not run: {ex}"}, **host_cpu())
         print(json.dumps(line), flush=True)
     g.free()
     if world > 1:

@@ -82,10 +82,14 @@ typedef struct {
 /* ------------------------------------------------------------------ graphs */
 
 /* Build a device graph from an edge list (src[e] -> dst[e], weight w[e]).
- * w may be NULL (all weights 1.0).  The device copy is an int32 CSR with
- * vertices relabelled by out-degree (descending), rows sorted by neighbour,
- * plus the transposed CSR for bottom-up BFS; results are reported in the
- * caller's original ids.  Replaces the per-call edge-list upload of
+ * w may be NULL (all weights 1.0); weights must be finite and >= 0 (NaN,
+ * infinite or negative weights are rejected with TRAV_ERR_BAD_ARG).  The
+ * device copy is an int32 CSR with vertices relabelled by out-degree
+ * (descending, ties by id), each row sorted by weight (-0.0 read as +0.0,
+ * equal weights in edge-list order) so the edges lighter than any delta form
+ * a prefix, plus the transposed CSR (rows sorted by source, with each
+ * in-edge's weight) for bottom-up BFS and SSSP pull rounds; results are
+ * reported in the caller's original ids.  Replaces the per-call edge-list upload of
  * SingleSourceShortestPaths::gpu_bellman_ford (algorithm/sssp/sssp.hpp:219-277)
  * and BFS::gpu_bfs (algorithm/bfs/bfs.hpp:212-254). */
 int trav_graph_from_edges(int32_t vertices, int64_t edges, const int32_t *src, const int32_t *dst,
@@ -149,9 +153,12 @@ int trav_graph_set_stream(trav_graph *g, void *stream);
 int trav_last_bfs_trace(trav_graph *g, uint8_t *dirs, int64_t *frontier, int32_t cap, int32_t *nsteps);
 
 /* Phase log of the last query (the last source of a batch): per grid-wide
- * phase, its kind (0 top-down, 1 bottom-up, 2 frontier-bitmap build,
- * 3 SSSP relaxation round, 4 SSSP bucket opening), the frontier size it
- * started from, its end time in microseconds after the query's initialisation
+ * phase, its kind (0 BFS top-down step, 1 BFS bottom-up step, 2 BFS
+ * frontier-bitmap build, 3 SSSP light relaxation round, 4 SSSP bucket
+ * opening, 5 SSSP heavy round pushing the heavy list's out-rows, 6 SSSP pull
+ * check listing the vertices a heavy edge could still improve, 7 SSSP heavy
+ * round pulling over those vertices' in-rows), the frontier size it started
+ * from, its end time in microseconds after the query's initialisation
  * and the cumulative out-edges expanded.  Up to cap entries; *n receives the
  * phase count.  New; the reference has no equivalent. */
 int trav_last_phase_log(trav_graph *g, uint8_t *kind, int64_t *size, double *end_us, int64_t *edges, int32_t cap,
@@ -192,7 +199,9 @@ int trav_bfs_el(const int32_t *src, const int32_t *dst, int32_t vertices, int64_
  *
  * row_offsets (V+1 int32), adj (E int32, ids in [0, V)) and levels (V int32,
  * written: hop level or -1) are device pointers in the caller's vertex ids;
- * the CSR is checked before use.  Runs on `stream` (a cudaStream_t; NULL =
+ * a pointer that is not device (or managed) memory is rejected with
+ * TRAV_ERR_BAD_ARG before any launch, and the CSR is checked on the GPU
+ * before use.  Runs on `stream` (a cudaStream_t; NULL =
  * the legacy default stream) and returns after the work has finished.
  * The first call on a device looks up the device address of the static array
  * (cudaGetSymbolAddress) once for that device; make that first call before
@@ -216,11 +225,40 @@ int trav_el_file_read(const char *path, int32_t unweighted, int32_t *vertices, i
 int trav_el_file_write(const char *path, int32_t directed, int32_t vertices, int64_t edges,
                        const int32_t *src, const int32_t *dst, const float *w);
 
+/* Read an adjacency-list binary file in the reference format
+ * (GraphStorageAPI::load_from_adjacency_list_bin_file,
+ * include/storage/graph_storage_API.hpp:69-111): the same 13-byte header
+ * (bool directed, int32 V, int64 E), then per vertex a Vertex<int> record
+ * {int32 id, int32 value}, an int32 connection count and that many
+ * {int32 dst, float32 w} records.  Call with offsets == NULL to get V, E and
+ * directed only; otherwise ids[V], values[V], offsets[V+1] (row v holds
+ * edges [offsets[v], offsets[v+1]) in file order, its source is ids[v]),
+ * dst[E] and w[E] are filled.  A file whose records do not add up to the
+ * header's E, ends inside a record or has bytes after the last one is
+ * rejected with TRAV_ERR_IO. */
+int trav_adj_file_read(const char *path, int32_t *vertices, int64_t *edges, int32_t *directed, int32_t *ids,
+                       int32_t *values, int64_t *offsets, int32_t *dst, float *w);
+
+/* Write the same format (GraphStorageAPI::save_to_adjacency_list_bin_file,
+ * include/storage/graph_storage_API.hpp:3-35) from the arrays
+ * trav_adj_file_read returns. */
+int trav_adj_file_write(const char *path, int32_t directed, int32_t vertices, int64_t edges, const int32_t *ids,
+                        const int32_t *values, const int64_t *offsets, const int32_t *dst, const float *w);
+
+/* Read a headerless file of {int32 src, int32 dst} pairs as the BFS sample's
+ * read_data_from_file does (sample/bfs.cpp:84-114): V = 2^vertices_pow, and
+ * the edge count is file_size / 12 -- the reference sizes it for 12-byte
+ * weighted records but reads 8-byte pairs, so it takes the first
+ * file_size / 12 pairs of the file, and that count is kept here.  Every
+ * weight is 1.0.  Call with src == NULL to get V and E only. */
+int trav_pairs_file_read(const char *path, int32_t vertices_pow, int32_t *vertices, int64_t *edges, int32_t *src,
+                         int32_t *dst, float *w);
+
 /* ------------------------------------------------------- learned schedule */
 
 /* Install the parameters of a schedule MLP on a handle (copied to the
  * device).  kind 0 = BFS direction (2 outputs: top-down, bottom-up);
- * kind 1 = SSSP bucket width (4 outputs: delta x 1, 4, 16, 64).  count must be
+ * kind 1 = SSSP bucket width (6 outputs: delta x 1, 4, 16, 64, 256, 1024).  count must be
  * trav_mlp_param_count(kind).  Layout: [W1 (32x10) | b1 (32) | W2 (32x32) |
  * b2 (32) | W3 (Ox32) | b3 (O)], row-major, tanh hidden units.  New; the
  * reference has no learned schedule. */
@@ -256,12 +294,30 @@ int trav_graph_set_capture(trav_graph *g, int32_t on);
  * reference. */
 int trav_set_grid(trav_graph *g, int32_t kind, int32_t ctas, int32_t *max_ctas);
 
+/* Limits of the following trav_bfs / trav_sssp queries on this handle (batch
+ * launches keep the defaults).  max_steps caps a query's
+ * steps (BFS levels; SSSP relaxation rounds plus bucket openings) below its
+ * default budget (BFS V + 1, SSSP 4V + 4096); 0 restores the default.
+ * timeout_ns bounds every wait of a grid barrier inside the persistent
+ * kernels; 0 restores the default of 10 s.  A query that runs out of either
+ * returns TRAV_ERR_TIMEOUT (trav_last_error says which) and leaves the
+ * handle usable.  The reference's counterpart is the V-iteration cap of
+ * bellman_ford_wrapper (algorithm/sssp/gpu/bellman_ford.cu:126); its BFS
+ * loop has none (algorithm/bfs/gpu/bfs.cu:69). */
+int trav_set_limits(trav_graph *g, int32_t max_steps, uint64_t timeout_ns);
+
+/* Fault injection for tests of the out-of-memory paths: after `after` more
+ * device allocations by this library succeed, the next one fails as
+ * cudaMalloc fails when the device is full (TRAV_ERR_OOM), once; -1 disarms.
+ * Process-wide.  No counterpart in the reference. */
+int trav_inject_alloc_failure(int32_t after);
+
 /* Force the schedule's decisions for the following queries of one kind on
  * this handle (used to time alternatives when building training traces):
  * decision i takes option plan[i] when plan[i] < 255 and follows the schedule
  * otherwise.  BFS decision i is the direction of step i (0 top-down, 1
  * bottom-up); SSSP decision i is the width option of the i-th bucket opening
- * (delta x 1, 4, 16, 64).  n == 0 clears the plan. */
+ * (0..5: delta x 1, 4, 16, 64, 256, 1024).  n == 0 clears the plan. */
 int trav_set_plan(trav_graph *g, int32_t kind, const uint8_t *plan, int32_t n);
 
 /* Decisions of the last query (the last source of a batch): per decision the

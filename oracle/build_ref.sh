@@ -1,16 +1,17 @@
 #!/usr/bin/env bash
 # Builds oracle/_ref/libtrav_ref.so: oracle/ref_harness.cpp compiled against the
-# reference library's headers where they lie (REF_ROOT, default
-# /root/reference).  Nothing is copied from the reference; the output goes only
-# to oracle/_ref/ (git-ignored, but shipped with the working tree so the CPU
-# baseline can run where the reference sources are absent).
+# reference library's headers where they lie.  The reference root is the first
+# argument or $REF_ROOT; without either, the existing oracle/_ref is kept.
+# Nothing is copied from the reference; the output goes only to oracle/_ref/
+# (git-ignored, but shipped with the working tree so the CPU baseline can run
+# where the reference sources are absent).
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF_ROOT="${REF_ROOT:-/root/reference}"
+REF_ROOT="${1:-${REF_ROOT:-}}"
 CUDA_HOME="${CUDA_HOME:-/usr/local/cuda}"
 OUT="$HERE/_ref"
-if [ ! -d "$REF_ROOT/algorithm" ]; then
-  echo "build_ref: reference sources not found at $REF_ROOT; keeping existing $OUT" >&2
+if [ -z "$REF_ROOT" ] || [ ! -d "$REF_ROOT/algorithm" ]; then
+  echo "build_ref: no reference sources given (argument or REF_ROOT); keeping existing $OUT" >&2
   exit 0
 fi
 mkdir -p "$OUT"

@@ -104,6 +104,9 @@ def ref():
         L.ref_gpu_transactions.argtypes = [vp, C.c_int]
         L.ref_gpu_transactions.restype = C.c_longlong
         L.ref_load_edges_list.restype = vp
+        L.ref_load_adjacency_list_as_el.argtypes = [C.c_char_p]
+        L.ref_load_adjacency_list_as_el.restype = vp
+        L.ref_graph_vertices.restype = C.c_int
         L.ref_wtime.restype = C.c_double
         _ref = L
     return _ref
@@ -234,6 +237,13 @@ class RefGraph:
     def csr(cls, V, offsets, adj, w):
         return cls(ref().ref_graph_csr(V, int(offsets[-1]), _c(offsets, np.int64), _c(adj, np.int32),
                                        _c(w, np.float32)), V, int(offsets[-1]))
+
+    @classmethod
+    def load_adjacency_list_as_el(cls, path):
+        """The reference's adjacency-list loader, then its conversion to an edge list."""
+        h = ref().ref_load_adjacency_list_as_el(path.encode())
+        assert h, f"reference loader refused {path}"
+        return cls(h, ref().ref_graph_vertices(h), ref().ref_graph_edges(h))
 
     def export_csr(self):
         off = np.empty(self.V + 1, np.int64)

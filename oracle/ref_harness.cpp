@@ -13,6 +13,7 @@
 //   BFS::cpu_parallel_bfs                         algorithm/bfs/bfs.hpp:117-208
 //   GraphGenerationAPI::R_MAT_parallel            include/test/generation/graph_generation_API.hpp:403-484
 //   GraphStorageAPI::{save,load}_*_bin_file       include/storage/graph_storage_API.hpp:3-160
+//   Graph::convert_to_edges_list                  include/graph_data_structures/graph.hpp:366-401
 //   Graph::convert_to_compressed_adjacency_list   include/graph_data_structures/graph.hpp:316-361
 //   GraphOptimizationAPI::optimize_graph_for_CPU  include/test/optimization/graph_optimization_API.hpp:173-224
 //   GraphOptimizationAPI::check_gpu_memory_transactions_count                             :229-266
@@ -155,6 +156,26 @@ void *ref_load_edges_list(const char *path)
 {
     RefGraph *g = new RefGraph(0, 0, EDGES_LIST, true);
     if (!GraphStorageAPI<int, float>::load_from_edges_list_bin_file(*g, std::string(path))) {
+        delete g;
+        return nullptr;
+    }
+    return g;
+}
+
+// Load an adjacency-list binary through the reference loader
+// (load_from_adjacency_list_bin_file, graph_storage_API.hpp:69-111) into an
+// adjacency-list graph, then convert it to an edge list the reference's way
+// (Graph::convert_to_edges_list, graph.hpp:366-401).
+void *ref_load_adjacency_list_as_el(const char *path)
+{
+    RefGraph *g = new RefGraph(0, 0, ADJACENCY_LIST, true);
+    try {
+        if (!GraphStorageAPI<int, float>::load_from_adjacency_list_bin_file(*g, std::string(path))) {
+            delete g;
+            return nullptr;
+        }
+        g->convert_to_edges_list();
+    } catch (const char *) {
         delete g;
         return nullptr;
     }

@@ -99,9 +99,9 @@ int ensure_teams(trav_batch *b, int teams)
     b->teams_alloc = 0;
     const TeamLayout L = team_layout(b);
     b->team_bytes = L.total;
-    TRY_CUDA(cudaMalloc(&b->team_mem, L.total * (size_t)teams));
-    TRY_CUDA(cudaMalloc(&b->d_teams, sizeof(TeamWs) * (size_t)teams));
-    TRY_CUDA(cudaMalloc(&b->ctl, sizeof(Ctl) * (size_t)teams));
+    TRY_CUDA(dev_malloc(&b->team_mem, L.total * (size_t)teams));
+    TRY_CUDA(dev_malloc(&b->d_teams, sizeof(TeamWs) * (size_t)teams));
+    TRY_CUDA(dev_malloc(&b->ctl, sizeof(Ctl) * (size_t)teams));
     std::vector<TeamWs> h((size_t)teams);
     for (int t = 0; t < teams; t++) {
         unsigned char *m = b->team_mem + L.total * (size_t)t;
@@ -181,7 +181,7 @@ int build_queries(trav_batch *b, const trav_query *qs, int32_t n, std::vector<Ba
             auto it = b->nlight.find(key);
             if (it == b->nlight.end()) {
                 int32_t *p = nullptr;
-                TRY_CUDA(cudaMalloc(&p, sizeof(int32_t) * (size_t)std::max<int32_t>(g->g.V, 1)));
+                TRY_CUDA(dev_malloc(&p, sizeof(int32_t) * (size_t)std::max<int32_t>(g->g.V, 1)));
                 it = b->nlight.emplace(key, p).first;
                 TRY(count_light(g->g, q.delta, p, b->st));
             }
@@ -266,7 +266,7 @@ int upload_queries(trav_batch *b, const trav_query *qs, int32_t n)
         cudaFree(b->d_q);
         b->d_q = nullptr;
         b->q_cap = 0;
-        TRY_CUDA(cudaMalloc(&b->d_q, sizeof(BatchQuery) * (size_t)n));
+        TRY_CUDA(dev_malloc(&b->d_q, sizeof(BatchQuery) * (size_t)n));
         b->q_cap = n;
     }
     if (n > 0) TRY_CUDA(cudaMemcpyAsync(b->d_q, d.data(), sizeof(BatchQuery) * (size_t)n, cudaMemcpyHostToDevice, b->st));
@@ -304,7 +304,7 @@ int trav_batch_create(trav_graph *const *graphs, int32_t n, trav_batch **out)
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_next, sizeof(unsigned));
+    if (e == cudaSuccess) e = dev_malloc(&b->d_next, sizeof(unsigned));
     if (e != cudaSuccess) {
         trav_batch_free(b);
         return cuda_fail(e, "trav_batch_create");

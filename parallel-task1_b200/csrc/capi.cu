@@ -4,6 +4,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
+#include <atomic>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -26,6 +27,34 @@ int cuda_fail(cudaError_t e, const char *what)
     if (e == cudaErrorMemoryAllocation) return TRAV_ERR_OOM;
     if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return TRAV_ERR_NO_DEVICE;
     return TRAV_ERR_CUDA;
+}
+
+// Allocations left before the injected failure (-1: none armed).
+static std::atomic<int64_t> g_alloc_fail_after{-1};
+
+cudaError_t dev_malloc_bytes(void **p, size_t bytes)
+{
+    int64_t left = g_alloc_fail_after.load();
+    while (left >= 0) {
+        if (g_alloc_fail_after.compare_exchange_weak(left, left - 1)) {
+            if (left == 0) {
+                *p = nullptr;
+                return cudaErrorMemoryAllocation;  // fires once, then the injection is disarmed
+            }
+            break;
+        }
+    }
+    return cudaMalloc(p, bytes);
+}
+
+bool is_device_ptr(const void *p)
+{
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 
 }  // namespace trav
@@ -63,16 +92,6 @@ int check_device()
     return TRAV_OK;
 }
 
-bool is_device_ptr(const void *p)
-{
-    cudaPointerAttributes at;
-    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
-}
-
 // Finish a new handle from a built device graph.
 int finish_handle(trav_graph *h)
 {
@@ -82,7 +101,7 @@ int finish_handle(trav_graph *h)
                             cudaMemcpyDeviceToHost));
     TRY(workspace_ensure(&h->ws, h->g, 1, h->st));
     for (int b = 0; b < 2; b++) {
-        TRY_CUDA(cudaMalloc(&h->staging[b], sizeof(float) * (size_t)(h->g.V > 0 ? h->g.V : 1)));
+        TRY_CUDA(dev_malloc(&h->staging[b], sizeof(float) * (size_t)(h->g.V > 0 ? h->g.V : 1)));
         TRY_CUDA(cudaEventCreateWithFlags(&h->done[b], cudaEventDisableTiming));
         TRY_CUDA(cudaEventCreateWithFlags(&h->copied[b], cudaEventDisableTiming));
     }
@@ -157,6 +176,8 @@ std::vector<unsigned char> capture_key(const trav_graph *g, int kind, const int3
     put(k, g->ws.item);
     put(k, g->ws.plan[kind]);
     put(k, g->ws.plan_len[kind]);
+    put(k, g->ws.max_steps);
+    put(k, g->ws.timeout_ns);
     put(k, g->st);
     put(k, g->ws.ctl);
     return k;
@@ -262,6 +283,13 @@ const char *trav_last_error(void) { return g_err.c_str(); }
 
 const char *trav_version(void) { return "trav-b200 0.1 (sm_100a)"; }
 
+int trav_inject_alloc_failure(int32_t after)
+{
+    if (after < -1) return bad("after must be >= -1");
+    g_alloc_fail_after.store(after);
+    return TRAV_OK;
+}
+
 int trav_graph_from_edges(int32_t vertices, int64_t edges, const int32_t *src, const int32_t *dst, const float *w,
                           int32_t mem, trav_graph **out)
 {
@@ -283,12 +311,12 @@ int trav_graph_from_edges(int32_t vertices, int64_t edges, const int32_t *src, c
     const int32_t *ps = src, *pd = dst;
     const float *pw = w;
     if (mem == TRAV_MEM_HOST && edges > 0) {
-        TRY_CUDA(cudaMalloc(&ds.p, sizeof(int32_t) * (size_t)edges));
-        TRY_CUDA(cudaMalloc(&dd.p, sizeof(int32_t) * (size_t)edges));
+        TRY_CUDA(dev_malloc(&ds.p, sizeof(int32_t) * (size_t)edges));
+        TRY_CUDA(dev_malloc(&dd.p, sizeof(int32_t) * (size_t)edges));
         TRY_CUDA(cudaMemcpyAsync(ds.p, src, sizeof(int32_t) * (size_t)edges, cudaMemcpyHostToDevice, h->st));
         TRY_CUDA(cudaMemcpyAsync(dd.p, dst, sizeof(int32_t) * (size_t)edges, cudaMemcpyHostToDevice, h->st));
         if (w) {
-            TRY_CUDA(cudaMalloc(&dw.p, sizeof(float) * (size_t)edges));
+            TRY_CUDA(dev_malloc(&dw.p, sizeof(float) * (size_t)edges));
             TRY_CUDA(cudaMemcpyAsync(dw.p, w, sizeof(float) * (size_t)edges, cudaMemcpyHostToDevice, h->st));
         }
         ps = ds.p;
@@ -323,9 +351,9 @@ int trav_graph_rmat(int32_t scale, int32_t avg, int32_t a, int32_t b, int32_t c,
     int32_t *ps = src, *pd = dst;
     float *pw = w;
     if (!src) {
-        TRY_CUDA(cudaMalloc(&ds.p, sizeof(int32_t) * (size_t)E));
-        TRY_CUDA(cudaMalloc(&dd.p, sizeof(int32_t) * (size_t)E));
-        TRY_CUDA(cudaMalloc(&dw.p, sizeof(float) * (size_t)E));
+        TRY_CUDA(dev_malloc(&ds.p, sizeof(int32_t) * (size_t)E));
+        TRY_CUDA(dev_malloc(&dd.p, sizeof(int32_t) * (size_t)E));
+        TRY_CUDA(dev_malloc(&dw.p, sizeof(float) * (size_t)E));
         ps = ds.p;
         pd = dd.p;
         pw = dw.p;
@@ -486,9 +514,9 @@ int trav_el_optimize(int32_t *src, int32_t *dst, float *w, int32_t vertices, int
     float *ww = w;
     const size_t bi = sizeof(int32_t) * (size_t)edges, bf = sizeof(float) * (size_t)edges;
     if (mem == TRAV_MEM_HOST) {
-        TRY_CUDA(cudaMalloc(&ds.p, bi));
-        TRY_CUDA(cudaMalloc(&dd.p, bi));
-        TRY_CUDA(cudaMalloc(&dw.p, bf));
+        TRY_CUDA(dev_malloc(&ds.p, bi));
+        TRY_CUDA(dev_malloc(&dd.p, bi));
+        TRY_CUDA(dev_malloc(&dw.p, bf));
         TRY_CUDA(cudaMemcpy(ds.p, src, bi, cudaMemcpyHostToDevice));
         TRY_CUDA(cudaMemcpy(dd.p, dst, bi, cudaMemcpyHostToDevice));
         TRY_CUDA(cudaMemcpy(dw.p, w, bf, cudaMemcpyHostToDevice));
@@ -522,8 +550,8 @@ int trav_el_gpu_transactions(const int32_t *src, const int32_t *dst, int32_t ver
     const int32_t *s = src, *d = dst;
     if (mem == TRAV_MEM_HOST) {
         const size_t bi = sizeof(int32_t) * (size_t)edges;
-        TRY_CUDA(cudaMalloc(&ds.p, bi));
-        TRY_CUDA(cudaMalloc(&dd.p, bi));
+        TRY_CUDA(dev_malloc(&ds.p, bi));
+        TRY_CUDA(dev_malloc(&dd.p, bi));
         TRY_CUDA(cudaMemcpy(ds.p, src, bi, cudaMemcpyHostToDevice));
         TRY_CUDA(cudaMemcpy(dd.p, dst, bi, cudaMemcpyHostToDevice));
         s = ds.p, d = dd.p;
@@ -560,6 +588,17 @@ int trav_set_grid(trav_graph *g, int32_t kind, int32_t ctas, int32_t *max_ctas)
     return TRAV_OK;
 }
 
+int trav_set_limits(trav_graph *g, int32_t max_steps, uint64_t timeout_ns)
+{
+    if (!g) return bad("graph handle is NULL");
+    if (max_steps < 0) return bad("max_steps must be >= 0 (0 = the default budget)");
+    TRY_CUDA(cudaSetDevice(g->device));
+    TRY_CUDA(cudaStreamSynchronize(g->st));
+    g->ws.max_steps = max_steps;
+    g->ws.timeout_ns = timeout_ns;
+    return TRAV_OK;
+}
+
 int trav_set_plan(trav_graph *g, int32_t kind, const uint8_t *plan, int32_t n)
 {
     if (!g) return bad("graph handle is NULL");
@@ -571,7 +610,7 @@ int trav_set_plan(trav_graph *g, int32_t kind, const uint8_t *plan, int32_t n)
     g->ws.plan[kind] = nullptr;
     g->ws.plan_len[kind] = 0;
     if (n == 0) return TRAV_OK;
-    TRY_CUDA(cudaMalloc(&g->ws.plan[kind], (size_t)n));
+    TRY_CUDA(dev_malloc(&g->ws.plan[kind], (size_t)n));
     TRY_CUDA(cudaMemcpy(g->ws.plan[kind], plan, (size_t)n, cudaMemcpyHostToDevice));
     g->ws.plan_len[kind] = n;
     return TRAV_OK;
@@ -654,7 +693,7 @@ int trav_mlp_set(trav_graph *g, int32_t kind, const float *params, int32_t count
     for (int32_t i = 0; i < count; i++)
         if (!std::isfinite(params[i])) return bad("MLP parameters must be finite");
     TRY_CUDA(cudaSetDevice(g->device));
-    if (!g->mlp[kind]) TRY_CUDA(cudaMalloc(&g->mlp[kind], sizeof(float) * (size_t)count));
+    if (!g->mlp[kind]) TRY_CUDA(dev_malloc(&g->mlp[kind], sizeof(float) * (size_t)count));
     TRY_CUDA(cudaMemcpy(g->mlp[kind], params, sizeof(float) * (size_t)count, cudaMemcpyHostToDevice));
     return TRAV_OK;
 }
@@ -676,7 +715,7 @@ static __global__ void gather_bits_kernel(unsigned *value, const float *d, const
 int trav_init_distances_f32(float *d, int32_t vertices, int32_t source)
 {
     TRY(check_device());
-    if (!d || vertices < 1) return bad("d must be a device array of vertices >= 1 floats");
+    if (!d || vertices < 1 || !is_device_ptr(d)) return bad("d must be a device array of vertices >= 1 floats");
     if (source < 0 || source >= vertices) return bad("source vertex out of range [0, V)");
     init_distances_kernel<<<(vertices + 255) / 256 < 4096 ? (vertices + 255) / 256 : 4096, 256>>>(d, vertices, source);
     TRY_CUDA(cudaGetLastError());
@@ -691,6 +730,8 @@ int trav_bellman_ford_el_f32(const int32_t *src, const int32_t *dst, const float
     if (!d || vertices < 1) return bad("d must be a device array of vertices >= 1 floats");
     if (source < 0 || source >= vertices) return bad("source vertex out of range [0, V)");
     if (edges < 0 || (edges > 0 && (!src || !dst || !w))) return bad("edge arrays must be device arrays of `edges` entries");
+    if (!is_device_ptr(d) || (edges > 0 && !(is_device_ptr(src) && is_device_ptr(dst) && is_device_ptr(w))))
+        return bad("src, dst, w and d must be device memory (the reference wrappers take device arrays)");
     if (edges >= (int64_t)INT32_MAX) {
         set_error("graph has 2^31 or more edges; the device CSR uses int32 offsets");
         return TRAV_ERR_OVERFLOW_INT32;
@@ -716,6 +757,8 @@ int trav_bfs_el(const int32_t *src, const int32_t *dst, int32_t vertices, int64_
     if (!visited || vertices < 1) return bad("visited must be a device array of vertices >= 1 bytes");
     if (source < 0 || source >= vertices) return bad("source vertex out of range [0, V)");
     if (edges < 0 || (edges > 0 && (!src || !dst))) return bad("edge arrays must be device arrays of `edges` entries");
+    if (!is_device_ptr(visited) || (edges > 0 && !(is_device_ptr(src) && is_device_ptr(dst))))
+        return bad("src, dst and visited must be device memory (the reference wrapper takes device arrays)");
     if (edges >= (int64_t)INT32_MAX) {
         set_error("graph has 2^31 or more edges; the device CSR uses int32 offsets");
         return TRAV_ERR_OVERFLOW_INT32;

@@ -31,7 +31,7 @@ namespace {
 template <class T>
 struct Buf {
     T *p = nullptr;
-    cudaError_t alloc(int64_t n) { return cudaMalloc((void **)&p, sizeof(T) * (size_t)(n > 0 ? n : 1)); }
+    cudaError_t alloc(int64_t n) { return dev_malloc((void **)&p, sizeof(T) * (size_t)(n > 0 ? n : 1)); }
     ~Buf() { if (p) cudaFree(p); }
 };
 

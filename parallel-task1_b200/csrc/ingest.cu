@@ -92,7 +92,8 @@ __global__ void loop_flags_kernel(const int32_t *__restrict__ src, const int32_t
         keep[e] = src[e] != dst[e];
 }
 
-// bad[0] |= 1 for an id out of range, 2 for a negative weight.
+// bad[0] |= 1 for an id out of range, 2 for a negative weight, 4 for a NaN or
+// infinite weight (the fp32 fixpoint is defined for finite weights >= 0).
 __global__ void validate_kernel(int32_t V, int64_t E, const int32_t *__restrict__ src,
                                 const int32_t *__restrict__ dst, const float *__restrict__ w, int *bad)
 {
@@ -100,7 +101,11 @@ __global__ void validate_kernel(int32_t V, int64_t E, const int32_t *__restrict_
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
         int s = src[e], t = dst[e];
         if (s < 0 || s >= V || t < 0 || t >= V) flag |= 1;
-        if (w && w[e] < 0.0f) flag |= 2;
+        if (w) {
+            const float x = w[e];
+            if (x < 0.0f) flag |= 2;
+            if (!isfinite(x)) flag |= 4;
+        }
     }
     flag = __reduce_or_sync(0xffffffffu, flag);
     if (flag && (threadIdx.x & 31) == 0) atomicOr(bad, flag);
@@ -207,7 +212,7 @@ __global__ void weight_sum_kernel(int64_t E, const float *__restrict__ w, double
 template <class T>
 struct DBuf {
     T *p = nullptr;
-    cudaError_t alloc(int64_t n) { return cudaMalloc((void **)&p, sizeof(T) * (size_t)(n > 0 ? n : 1)); }
+    cudaError_t alloc(int64_t n) { return dev_malloc((void **)&p, sizeof(T) * (size_t)(n > 0 ? n : 1)); }
     ~DBuf() { if (p) cudaFree(p); }
     T *release() { T *q = p; p = nullptr; return q; }
 };
@@ -280,6 +285,7 @@ int validate_edges(int32_t V, int64_t E, const int32_t *d_src, const int32_t *d_
     TRY_CUDA(cudaStreamSynchronize(st));
     if (h & 1) { set_error("edge list holds a vertex id outside [0, V)"); return TRAV_ERR_BAD_ARG; }
     if (h & 2) { set_error("edge list holds a negative weight (only weights >= 0 are supported)"); return TRAV_ERR_BAD_ARG; }
+    if (h & 4) { set_error("edge list holds a NaN or infinite weight (weights must be finite)"); return TRAV_ERR_BAD_ARG; }
     return TRAV_OK;
 }
 

@@ -198,13 +198,13 @@ void launch_grad(int O, int nblk, MlpDev &d, int n)
 
 int upload(MlpDev &d, int P, const float *params, const float *x, const int32_t *labels, int n, int nblk)
 {
-    TRY_CUDA(cudaMalloc(&d.p, sizeof(float) * P));
-    TRY_CUDA(cudaMalloc(&d.g, sizeof(float) * P));
-    TRY_CUDA(cudaMalloc(&d.x, sizeof(float) * (size_t)n * kFeat));
-    TRY_CUDA(cudaMalloc(&d.y, sizeof(int) * (size_t)n));
-    TRY_CUDA(cudaMalloc(&d.partial, sizeof(float) * (size_t)nblk * P));
-    TRY_CUDA(cudaMalloc(&d.lpart, sizeof(float) * (size_t)nblk));
-    TRY_CUDA(cudaMalloc(&d.loss, sizeof(float)));
+    TRY_CUDA(dev_malloc(&d.p, sizeof(float) * P));
+    TRY_CUDA(dev_malloc(&d.g, sizeof(float) * P));
+    TRY_CUDA(dev_malloc(&d.x, sizeof(float) * (size_t)n * kFeat));
+    TRY_CUDA(dev_malloc(&d.y, sizeof(int) * (size_t)n));
+    TRY_CUDA(dev_malloc(&d.partial, sizeof(float) * (size_t)nblk * P));
+    TRY_CUDA(dev_malloc(&d.lpart, sizeof(float) * (size_t)nblk));
+    TRY_CUDA(dev_malloc(&d.loss, sizeof(float)));
     TRY_CUDA(cudaMemcpy(d.p, params, sizeof(float) * P, cudaMemcpyHostToDevice));
     TRY_CUDA(cudaMemcpy(d.x, x, sizeof(float) * (size_t)n * kFeat, cudaMemcpyHostToDevice));
     TRY_CUDA(cudaMemcpy(d.y, labels, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice));
@@ -267,8 +267,8 @@ extern "C" int trav_mlp_train(int32_t kind, float *params, const float *x, const
     MlpDev d;
     rc = upload(d, P, params, x, labels, n, nblk);
     if (rc) return rc;
-    TRY_CUDA(cudaMalloc(&d.m, sizeof(float) * P));
-    TRY_CUDA(cudaMalloc(&d.v, sizeof(float) * P));
+    TRY_CUDA(dev_malloc(&d.m, sizeof(float) * P));
+    TRY_CUDA(dev_malloc(&d.v, sizeof(float) * P));
     TRY_CUDA(cudaMemset(d.m, 0, sizeof(float) * P));
     TRY_CUDA(cudaMemset(d.v, 0, sizeof(float) * P));
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;

@@ -22,6 +22,7 @@ constexpr int kMaxTrace = 4096;   // steps recorded per query
 constexpr int kMaxDec = 1024;     // schedule decisions recorded per query
 constexpr int kDecFeat = 10;      // features per decision (the schedule MLP's input width)
 constexpr int kSlots = 4;         // ring of per-phase counter slots
+constexpr unsigned long long kDefaultTimeoutNs = 10ull * 1000000000ull;  // grid-barrier wait limit (10 s)
 // Row-class flags in the low bits of an SSSP distance word (dist_bits << 32 |
 // round << kClsBits | flags): which parts of the vertex's out-row are non-empty
 // and which are longer than kSmallDeg.  They depend only on the graph and
@@ -122,6 +123,8 @@ struct Workspace {
     int grid[2] = {0, 0};              // CTAs of the BFS / SSSP launches (0 = as many as fit)
     int small_deg = kSmallDeg;         // expansion thresholds of the launches (see TravArgs)
     int item = kItem;
+    int max_steps = 0;                 // step budget of a query; 0 = the default (see launch_bfs / launch_sssp)
+    unsigned long long timeout_ns = 0;  // bounded wait of a grid barrier; 0 = kDefaultTimeoutNs
 };
 
 // Arguments of the persistent kernels (passed by value).
@@ -218,6 +221,19 @@ __device__ __forceinline__ int team_threads(const TravArgs &a) { return a.ctas *
 // ---- host-side helpers (capi.cu) ----
 void set_error(const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
+// True when p is device or managed memory of the current context (a pointer
+// the kernels may dereference); false for host memory and unknown pointers.
+bool is_device_ptr(const void *p);
+
+// Every device allocation of the library goes through dev_malloc: cudaMalloc,
+// unless a test armed trav_inject_alloc_failure, in which case the armed
+// allocation fails with cudaErrorMemoryAllocation as cudaMalloc would.
+cudaError_t dev_malloc_bytes(void **p, size_t bytes);
+template <class T>
+inline cudaError_t dev_malloc(T **p, size_t bytes)
+{
+    return dev_malloc_bytes(reinterpret_cast<void **>(p), bytes);
+}
 
 // ingest.cu
 int build_graph_device(int32_t V, int64_t E, const int32_t *d_src, const int32_t *d_dst, const float *d_w,

@@ -1834,7 +1834,7 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
         cudaFree(ws->ctl);
         ws->ctl = nullptr;
         ws->ctl_cap = 0;
-        TRY_CUDA(cudaMalloc(&ws->ctl, sizeof(Ctl) * (size_t)nqueries));
+        TRY_CUDA(dev_malloc(&ws->ctl, sizeof(Ctl) * (size_t)nqueries));
         ws->ctl_cap = nqueries;
         return TRAV_OK;
     }
@@ -1843,23 +1843,23 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
     const int64_t W = (V + 31) / 32;
     ws->V = g.V;
     ws->chunk_cap = V + g.E / kMinItem + 1;
-    TRY_CUDA(cudaMalloc(&ws->value, sizeof(unsigned long long) * V));
+    TRY_CUDA(dev_malloc(&ws->value, sizeof(unsigned long long) * V));
 
-    TRY_CUDA(cudaMalloc(&ws->visited, sizeof(unsigned) * W));
-    TRY_CUDA(cudaMalloc(&ws->front[0], sizeof(unsigned) * W));
-    TRY_CUDA(cudaMalloc(&ws->front[1], sizeof(unsigned) * W));
+    TRY_CUDA(dev_malloc(&ws->visited, sizeof(unsigned) * W));
+    TRY_CUDA(dev_malloc(&ws->front[0], sizeof(unsigned) * W));
+    TRY_CUDA(dev_malloc(&ws->front[1], sizeof(unsigned) * W));
     for (int i = 0; i < 2; i++) {
-        TRY_CUDA(cudaMalloc(&ws->queue[i], sizeof(int32_t) * V));
-        TRY_CUDA(cudaMalloc(&ws->far[i], sizeof(int32_t) * V));
+        TRY_CUDA(dev_malloc(&ws->queue[i], sizeof(int32_t) * V));
+        TRY_CUDA(dev_malloc(&ws->far[i], sizeof(int32_t) * V));
     }
-    TRY_CUDA(cudaMalloc(&ws->nlight, sizeof(int32_t) * V));
+    TRY_CUDA(dev_malloc(&ws->nlight, sizeof(int32_t) * V));
     for (int i = 0; i < 2; i++) {
-        TRY_CUDA(cudaMalloc(&ws->hq[i], sizeof(int32_t) * V));
-        TRY_CUDA(cudaMalloc(&ws->hchunks[i], sizeof(int2) * ws->chunk_cap));
+        TRY_CUDA(dev_malloc(&ws->hq[i], sizeof(int32_t) * V));
+        TRY_CUDA(dev_malloc(&ws->hchunks[i], sizeof(int2) * ws->chunk_cap));
     }
-    TRY_CUDA(cudaMalloc(&ws->chunks[0], sizeof(int2) * ws->chunk_cap));
-    TRY_CUDA(cudaMalloc(&ws->chunks[1], sizeof(int2) * ws->chunk_cap));
-    TRY_CUDA(cudaMalloc(&ws->ctl, sizeof(Ctl) * (size_t)nqueries));
+    TRY_CUDA(dev_malloc(&ws->chunks[0], sizeof(int2) * ws->chunk_cap));
+    TRY_CUDA(dev_malloc(&ws->chunks[1], sizeof(int2) * ws->chunk_cap));
+    TRY_CUDA(dev_malloc(&ws->ctl, sizeof(Ctl) * (size_t)nqueries));
     ws->ctl_cap = nqueries;
     ws->nlight_delta = -1.0f;
     return TRAV_OK;
@@ -1918,7 +1918,7 @@ static TravArgs make_args(const DevGraph &g, Workspace *ws)
     a.chunks = ws->chunks[0];
     a.chunks0 = ws->chunks[0];
     a.chunks1 = ws->chunks[1];
-    a.timeout_ns = 10ull * 1000000000ull;
+    a.timeout_ns = ws->timeout_ns ? ws->timeout_ns : kDefaultTimeoutNs;
     a.mean_w = g.mean_w;
     a.max_deg = g.max_out_degree;
     a.cta0 = 0;
@@ -1935,6 +1935,7 @@ int launch_bfs(const DevGraph &g, Workspace *ws, int q, int32_t source_new, cons
     a.ctl = ws->ctl + q;
     a.source = source_new;
     a.max_steps = g.V + 1;
+    if (ws->max_steps > 0 && ws->max_steps < a.max_steps) a.max_steps = ws->max_steps;
     a.alpha = o.alpha;
     a.beta = o.beta;
     a.force_dir = o.force_direction;
@@ -1954,6 +1955,7 @@ int launch_sssp(const DevGraph &g, Workspace *ws, int q, int32_t source_new, flo
     a.ctl = ws->ctl + q;
     a.source = source_new;
     a.max_steps = (int32_t)std::min<int64_t>(4 * (int64_t)g.V + 4096, kMaxRounds - 2);
+    if (ws->max_steps > 0 && ws->max_steps < a.max_steps) a.max_steps = ws->max_steps;
     a.force_dir = -1;
     a.delta = (delta > 0.0f && std::isfinite(delta)) ? delta : INFINITY;
     if (source_new < 0) {
@@ -1983,7 +1985,7 @@ int query_bytes(const DevGraph &g, Workspace *ws, int q, int kind, int64_t *byte
                 int64_t *reached_edges, cudaStream_t st)
 {
     unsigned long long *acc = nullptr;
-    TRY_CUDA(cudaMalloc(&acc, sizeof(unsigned long long) * 3));
+    TRY_CUDA(dev_malloc(&acc, sizeof(unsigned long long) * 3));
     TRY_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * 3, st));
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -2113,6 +2115,13 @@ extern "C" int trav_bfs_csr_noalloc(const int32_t *row_offsets, const int32_t *a
         set_error("trav_bfs_csr_noalloc: row_offsets, adj and levels must be device arrays");
         return TRAV_ERR_BAD_ARG;
     }
+    // The CSR check below runs on the GPU, so a host pointer must be caught
+    // here, before anything is launched on it.
+    if (!is_device_ptr(row_offsets) || !is_device_ptr(levels) || (edges > 0 && !is_device_ptr(adj))) {
+        set_error("trav_bfs_csr_noalloc: row_offsets, adj and levels must be device (or managed) memory of the "
+                  "current device");
+        return TRAV_ERR_BAD_ARG;
+    }
     if (vertices < 1 || vertices > kNoAllocMaxVertices || edges < 0 || edges > kNoAllocMaxEdges) {
         set_error("trav_bfs_csr_noalloc: needs 1 <= vertices <= 262144 and 0 <= edges <= 16777216 (its 8 MiB "
                   "static scratch); use trav_bfs for larger graphs");
@@ -2184,15 +2193,16 @@ extern "C" int trav_bfs_csr_noalloc(const int32_t *row_offsets, const int32_t *a
     a.source = source;
     a.max_steps = vertices + 1;
     a.force_dir = 0;
-    a.timeout_ns = 10ull * 1000000000ull;
+    a.timeout_ns = kDefaultTimeoutNs;
     a.cta0 = 0;
     a.ctas = sms * per;
     a.small_deg = kSmallDeg;
     a.item = kItem;
     void *params[] = {&a, &levels};
     TRY_CUDA(cudaLaunchCooperativeKernel((void *)bfs_csr_noalloc_kernel, dim3(sms * per), dim3(kBlock), params, 0, st));
-    TRY_CUDA(cudaStreamSynchronize(st));
+    // the status is read on the caller's stream, so no other stream is waited for
     Ctl h;
-    TRY_CUDA(cudaMemcpy(&h, a.ctl, offsetof(Ctl, slot), cudaMemcpyDeviceToHost));
+    TRY_CUDA(cudaMemcpyAsync(&h, a.ctl, offsetof(Ctl, slot), cudaMemcpyDeviceToHost, st));
+    TRY_CUDA(cudaStreamSynchronize(st));
     return device_timeout_err(h, "trav_bfs_csr_noalloc");
 }

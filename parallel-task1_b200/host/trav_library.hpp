@@ -4,6 +4,9 @@
 //
 //   GraphStorageAPI::load_from_edges_list_bin_file / save_to_edges_list_bin_file
 //       include/storage/graph_storage_API.hpp:39-65, 114-160
+//   GraphStorageAPI::load_from_adjacency_list_bin_file / save_to_adjacency_list_bin_file
+//       include/storage/graph_storage_API.hpp:3-35, 69-111
+//   read_data_from_file (headerless pairs)        sample/bfs.cpp:84-114
 //   GraphGenerationAPI::R_MAT_parallel
 //       include/test/generation/graph_generation_API.hpp:403-484
 //   SingleSourceShortestPaths::gpu_bellman_ford   algorithm/sssp/sssp.hpp:219-277
@@ -62,6 +65,73 @@ struct GraphStorageAPI {
     {
         return trav_el_file_write(file_name.c_str(), g.directed, g.vertices_count, g.get_edges_count(),
                                   g.src_ids.data(), g.dst_ids.data(), g.weights.data()) == TRAV_OK;
+    }
+
+    // Adjacency-list binary: rows in file order become edges grouped by
+    // source (the order the reference's conversion to an edge list gives).
+    static bool load_from_adjacency_list_bin_file(EdgesList &g, const std::string &file_name)
+    {
+        int32_t V = 0, directed = 1;
+        int64_t E = 0;
+        if (trav_adj_file_read(file_name.c_str(), &V, &E, &directed, nullptr, nullptr, nullptr, nullptr, nullptr) !=
+            TRAV_OK)
+            return false;
+        std::vector<int32_t> ids((size_t)V), values((size_t)V), dst((size_t)E);
+        std::vector<int64_t> off((size_t)V + 1);
+        std::vector<float> w((size_t)E);
+        if (trav_adj_file_read(file_name.c_str(), &V, &E, &directed, ids.data(), values.data(), off.data(), dst.data(),
+                               w.data()) != TRAV_OK)
+            return false;
+        g.vertices_count = V;
+        g.directed = directed != 0;
+        g.src_ids.resize((size_t)E);
+        for (int32_t v = 0; v < V; v++)
+            for (int64_t e = off[(size_t)v]; e < off[(size_t)v + 1]; e++) g.src_ids[(size_t)e] = ids[(size_t)v];
+        g.dst_ids = std::move(dst);
+        g.weights = std::move(w);
+        return true;
+    }
+
+    // Rows of vertices 0..V-1 (vertex values 0), each in edge-list order.
+    static bool save_to_adjacency_list_bin_file(const EdgesList &g, const std::string &file_name)
+    {
+        const int32_t V = g.vertices_count;
+        const int64_t E = g.get_edges_count();
+        std::vector<int64_t> off((size_t)V + 1, 0);
+        for (int64_t e = 0; e < E; e++) {
+            const int32_t s = g.src_ids[(size_t)e];
+            if (s < 0 || s >= V) return false;
+            off[(size_t)s + 1]++;
+        }
+        for (int32_t v = 0; v < V; v++) off[(size_t)v + 1] += off[(size_t)v];
+        std::vector<int64_t> at(off.begin(), off.end() - 1);
+        std::vector<int32_t> dst((size_t)E), ids((size_t)V), values((size_t)V, 0);
+        std::vector<float> w((size_t)E);
+        for (int64_t e = 0; e < E; e++) {
+            const int64_t k = at[(size_t)g.src_ids[(size_t)e]]++;
+            dst[(size_t)k] = g.dst_ids[(size_t)e];
+            w[(size_t)k] = g.weights[(size_t)e];
+        }
+        for (int32_t v = 0; v < V; v++) ids[(size_t)v] = v;
+        return trav_adj_file_write(file_name.c_str(), g.directed, V, E, ids.data(), values.data(), off.data(),
+                                   dst.data(), w.data()) == TRAV_OK;
+    }
+
+    // The BFS sample's headerless {int32, int32} pairs: V = 2^vertices_pow,
+    // the first file_size / 12 pairs, weight 1.0 each.
+    static bool read_data_from_file(EdgesList &g, const std::string &file_name, int vertices_pow)
+    {
+        int32_t V = 0;
+        int64_t E = 0;
+        if (trav_pairs_file_read(file_name.c_str(), vertices_pow, &V, &E, nullptr, nullptr, nullptr) != TRAV_OK)
+            return false;
+        g.vertices_count = V;
+        g.directed = true;
+        g.src_ids.resize((size_t)E);
+        g.dst_ids.resize((size_t)E);
+        g.weights.resize((size_t)E);
+        return trav_pairs_file_read(file_name.c_str(), vertices_pow, &V, &E, g.src_ids.data(), g.dst_ids.data(),
+                                    g.weights.data()) == TRAV_OK;
     }
 };
 

@@ -51,7 +51,8 @@ EXPORTS = [
     "trav_bfs_csr_noalloc", "trav_last_phase_log", "trav_mlp_loss_grad", "trav_mlp_train", "trav_set_plan",
     "trav_last_decisions", "trav_set_grid", "trav_batch_create", "trav_batch_free", "trav_batch_run",
     "trav_batch_autotune", "trav_batch_set_shape", "trav_batch_get_shape", "trav_graph_set_capture",
-    "trav_el_optimize", "trav_el_gpu_transactions",
+    "trav_el_optimize", "trav_el_gpu_transactions", "trav_adj_file_read", "trav_adj_file_write",
+    "trav_pairs_file_read", "trav_set_limits", "trav_inject_alloc_failure",
 ]
 
 
@@ -114,6 +115,9 @@ def lib():
         L.trav_bfs_el.argtypes = [vp, vp, i32, i64, vp, i32]
         L.trav_el_file_read.argtypes = [C.c_char_p, i32, C.POINTER(i32), C.POINTER(i64), C.POINTER(i32), vp, vp, vp]
         L.trav_el_file_write.argtypes = [C.c_char_p, i32, i32, i64, vp, vp, vp]
+        L.trav_adj_file_read.argtypes = [C.c_char_p, C.POINTER(i32), C.POINTER(i64), C.POINTER(i32)] + [vp] * 5
+        L.trav_adj_file_write.argtypes = [C.c_char_p, i32, i32, i64] + [vp] * 5
+        L.trav_pairs_file_read.argtypes = [C.c_char_p, i32, C.POINTER(i32), C.POINTER(i64), vp, vp, vp]
         L.trav_mlp_set.argtypes = [vp, i32, vp, i32]
         L.trav_set_grid.argtypes = [vp, i32, i32, C.POINTER(i32)]
         L.trav_graph_set_capture.argtypes = [vp, i32]
@@ -135,6 +139,8 @@ def lib():
         L.trav_mlp_loss_grad.argtypes = [i32, vp, vp, vp, i32, vp, C.POINTER(f32)]
         L.trav_mlp_train.argtypes = [i32, vp, vp, vp, i32, i32, f32, C.POINTER(f32)]
         L.trav_set_plan.argtypes = [vp, i32, vp, i32]
+        L.trav_set_limits.argtypes = [vp, i32, C.c_uint64]
+        L.trav_inject_alloc_failure.argtypes = [i32]
         L.trav_last_decisions.argtypes = [vp, vp, vp, vp, vp, vp, i32, C.POINTER(i32)]
         _lib = L
     return _lib
@@ -294,6 +300,10 @@ class Graph:
         _check(lib().trav_set_grid(self._h, kind, ctas, C.byref(most)))
         return most.value
 
+    def set_limits(self, max_steps: int = 0, timeout_ns: int = 0):
+        """Step budget and grid-barrier wait limit of later queries (0 = the defaults)."""
+        _check(lib().trav_set_limits(self._h, max_steps, timeout_ns))
+
     def set_plan(self, kind: int, plan=None):
         """Force decisions of later queries of `kind` (0 BFS, 1 SSSP); entries of 255 follow the schedule."""
         p = np.ascontiguousarray(plan if plan is not None else [], np.uint8)
@@ -401,6 +411,11 @@ def bfs_wrapper(src, dst, V: int, E: int, visited, source: int):
     _check(lib().trav_bfs_el(_ptr(src), _ptr(dst), V, E, _ptr(visited), source))
 
 
+def inject_alloc_failure(after: int):
+    """Test hook: the allocation after `after` more successful ones fails (TRAV_ERR_OOM), once; -1 disarms."""
+    _check(lib().trav_inject_alloc_failure(after))
+
+
 def bfs_csr_noalloc(row_offsets, adj, V: int, E: int, source: int, levels, stream=None):
     """Top-down BFS over a device CSR (CUDA int32 tensors) into `levels`, allocating nothing.
 
@@ -432,6 +447,52 @@ def write_edges_list(path: str, V: int, src, dst, w, directed: bool = True):
     w = np.ascontiguousarray(w, np.float32)
     _check(lib().trav_el_file_write(path.encode(), int(directed), V, len(src), src.ctypes.data, dst.ctypes.data,
                                     w.ctypes.data))
+
+
+def read_adjacency_list(path: str):
+    """The reference's adjacency-list binary: (ids, values, offsets, dst, w, V, directed); row v's edges are
+    dst/w[offsets[v]:offsets[v+1]] in file order and its source vertex is ids[v]."""
+    V, E, D = C.c_int32(), C.c_int64(), C.c_int32()
+    p = path.encode()
+    _check(lib().trav_adj_file_read(p, C.byref(V), C.byref(E), C.byref(D), None, None, None, None, None))
+    ids = np.empty(V.value, np.int32)
+    values = np.empty(V.value, np.int32)
+    off = np.empty(V.value + 1, np.int64)
+    dst = np.empty(max(E.value, 1), np.int32)
+    w = np.empty(max(E.value, 1), np.float32)
+    _check(lib().trav_adj_file_read(p, C.byref(V), C.byref(E), C.byref(D), ids.ctypes.data, values.ctypes.data,
+                                    off.ctypes.data, dst.ctypes.data, w.ctypes.data))
+    return ids, values, off, dst[: E.value], w[: E.value], V.value, bool(D.value)
+
+
+def write_adjacency_list(path: str, ids, values, offsets, dst, w, directed: bool = True):
+    ids = np.ascontiguousarray(ids, np.int32)
+    values = np.ascontiguousarray(values, np.int32)
+    offsets = np.ascontiguousarray(offsets, np.int64)
+    dst = np.ascontiguousarray(dst, np.int32)
+    w = np.ascontiguousarray(w, np.float32)
+    _check(lib().trav_adj_file_write(path.encode(), int(directed), len(ids), int(offsets[-1]), ids.ctypes.data,
+                                     values.ctypes.data, offsets.ctypes.data, dst.ctypes.data, w.ctypes.data))
+
+
+def adjacency_to_edges(ids, offsets, dst, w):
+    """Edge list (src, dst, w) of an adjacency list, rows in file order."""
+    src = np.repeat(np.asarray(ids, np.int32), np.diff(np.asarray(offsets, np.int64)))
+    return src, np.asarray(dst, np.int32), np.asarray(w, np.float32)
+
+
+def read_pairs(path: str, vertices_pow: int):
+    """Headerless {int32 src, int32 dst} pairs as the reference's BFS sample reads them: (src, dst, w, V) with
+    V = 2^vertices_pow, the first file_size / 12 pairs and every weight 1.0."""
+    V, E = C.c_int32(), C.c_int64()
+    p = path.encode()
+    _check(lib().trav_pairs_file_read(p, vertices_pow, C.byref(V), C.byref(E), None, None, None))
+    src = np.empty(max(E.value, 1), np.int32)
+    dst = np.empty(max(E.value, 1), np.int32)
+    w = np.empty(max(E.value, 1), np.float32)
+    _check(lib().trav_pairs_file_read(p, vertices_pow, C.byref(V), C.byref(E), src.ctypes.data, dst.ctypes.data,
+                                      w.ctypes.data))
+    return src[: E.value], dst[: E.value], w[: E.value], V.value
 
 
 class Batch:

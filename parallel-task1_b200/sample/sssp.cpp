@@ -4,7 +4,10 @@
 // as the reference's loop does (sample/sssp.cpp:117-120), printing the
 // GPU-only performance of each run like gpu_bellman_ford (sssp.hpp:274).
 //
-//   sssp <graph.el> [sources=10] [delta=0 (Bellman-Ford)]
+//   sssp <graph.el> [sources=10] [delta=0 (Bellman-Ford)] [out.bin]
+//
+// With out.bin, each run appends its int32 source and the V float distances
+// (caller ids, FLT_MAX unreachable) to that file.
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -23,6 +26,8 @@ int main(int argc, char *argv[])
         std::string file_name = argv[1];
         int runs = argc > 2 ? atoi(argv[2]) : 10;
         float delta = argc > 3 ? (float)atof(argv[3]) : 0.0f;
+        FILE *out = nullptr;
+        if (argc > 4 && !(out = fopen(argv[4], "wb"))) throw "Error: cannot create the output file";
         EdgesList graph;
         if (!GraphStorageAPI::load_from_edges_list_bin_file(graph, file_name)) throw "Error: no such graph file";
         printf("graph loaded!\n");
@@ -37,8 +42,12 @@ int main(int argc, char *argv[])
             double mteps = operation.gpu_bellman_ford(dg, result.data(), source_vertex, delta);
             printf("GPU-only perfomance: %f MTEPS (source %d)\n", mteps, source_vertex);
             avg += mteps;
+            if (out && (fwrite(&source_vertex, 4, 1, out) != 1 ||
+                        fwrite(result.data(), 4, result.size(), out) != result.size()))
+                throw "Error: writing the output file failed";
         }
         if (runs > 0) printf("avg perfomance: %f MTEPS\n", avg / runs);
+        if (out) fclose(out);
     } catch (const char *error) {
         printf("%s\n", error);
         return 1;

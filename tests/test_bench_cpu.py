@@ -28,3 +28,32 @@ def test_e2e_parts_cover_the_sources_in_order(n):
     assert len(cut) - 1 <= 4
     if n == 64:
         assert cut == [0, 24, 44, 58, 64]
+
+
+def test_cpu_baseline_parity_record_compares_bits():
+    """The CPU-baseline leg compares the reference's results with the GPU step's: here the step's results are
+    stood in for by the oracle's (equal), then by the oracle's with one distance bit flipped (not equal)."""
+    if not O.ref_available():
+        pytest.skip("oracle/_ref is not built")
+    import numpy as np
+
+    a = argparse.Namespace(scale=10, ef=8, seed=1, sources=3)
+    V = 1 << a.scale
+    s, d, w = O.rmat(a.scale, a.ef, (57, 19, 19, 5), seed=a.seed, drop_self_loops=True)
+    srcs = bench.pick_sources(np.bincount(s, minlength=V), a.sources, a.seed)
+    lv = np.stack([O.bfs_levels(V, s, d, int(x)) for x in srcs])
+    di = np.stack([O.dijkstra(V, s, d, w, int(x)) for x in srcs])
+    _, _, _, _, parity = bench.cpu_reference_run(a, 0.05, levels=lv, dist=di)
+    assert parity["sources"] >= 1 and parity["equal"] is True
+    bad = di.copy()
+    bad[:, np.flatnonzero(lv[0] > 0)[0]] = np.nextafter(bad[:, np.flatnonzero(lv[0] > 0)[0]], np.float32(2))
+    _, _, _, _, parity = bench.cpu_reference_run(a, 0.05, levels=lv, dist=bad)
+    assert parity["sources"] >= 1 and parity["equal"] is False
+
+
+def test_both_arms_print_the_same_config():
+    a = argparse.Namespace(scale=23, ef=32, seed=1, sources=64, delta=0.1)
+    c = bench.bench_config(a, 1 << 23, 268431728, 1)
+    assert c == bench.bench_config(a, 1 << 23, 268431728, 1)
+    assert "delta 0.1" in c["workload"] and "delta-stepping" not in c["workload"]
+    assert set(bench.host_cpu()) == {"cpu_model", "physical_cores", "logical_cpus"}

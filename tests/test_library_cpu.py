@@ -95,3 +95,29 @@ def test_no_device_is_a_clean_error():
     with pytest.raises(T.TravError) as e:
         T.Graph.from_edges(4, np.array([0, 1]), np.array([1, 2]), np.array([1.0, 1.0]))
     assert e.value.code == T.TRAV_ERR_NO_DEVICE
+
+
+def test_overflow_int32_is_rejected_before_any_device_access():
+    """Graphs of 2^31 or more edges do not fit the device CSR's int32 offsets: rejected from the sizes alone,
+    with pointers that are never dereferenced (the reference's bfs_kernel would index them with an int)."""
+    import ctypes as C
+
+    L = T.lib()
+    h = C.c_void_p()
+    dummy = C.c_void_p(16)  # never read: the size check comes first
+    rc = L.trav_graph_from_edges(4, 1 << 31, dummy, dummy, dummy, T.MEM_HOST, C.byref(h))
+    assert rc == T.TRAV_ERR_OVERFLOW_INT32 and not h.value
+    assert b"2^31" in L.trav_last_error()
+    e = C.c_int64()
+    rc = L.trav_graph_rmat(26, 32, 57, 19, 19, 5, 1, 1, None, None, None, C.byref(e), C.byref(h))
+    assert rc == T.TRAV_ERR_OVERFLOW_INT32 and not h.value
+
+
+def test_noalloc_bfs_refuses_host_pointers_without_launching():
+    """The allocation-free BFS checks that its arrays are device memory before its CSR check runs on the GPU."""
+    off = np.array([0, 1, 1], np.int32)
+    adj = np.array([1], np.int32)
+    lv = np.empty(2, np.int32)
+    with pytest.raises(T.TravError) as e:
+        T.bfs_csr_noalloc(off, adj, 2, 1, 0, lv)
+    assert e.value.code == T.TRAV_ERR_BAD_ARG and "device" in str(e.value)
