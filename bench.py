@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--delta", type=float, default=0.1)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference's own GPU path")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched many-graph measurement")
     ap.add_argument("--batched-only", action="store_true", help="run only the batched many-graph measurement")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="target seconds of CPU baseline work")
@@ -288,6 +289,50 @@ def cpu_reference_run(a, seconds, levels=None, dist=None):
         ref.free()
 
 
+def reference_gpu_run(a, cap_s: float = 90.0):
+    """The reference's own GPU path (its bellman_ford.cu and bfs.cu built unchanged for sm_100a, oracle/_ref) on
+    the same graph and sources: per source, bfs_wrapper then init_distances_wrapper + bellman_ford_wrapper on an
+    edge list resident in device memory, timed as the reference times them (host clock around the wrappers,
+    uploads excluded).  Stops after cap_s seconds of wrapper time and reports the sources it finished."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    if not O.refgpu_available():
+        return {"unavailable": "oracle/_ref/libtrav_refgpu.so is not built (needs the reference sources)"}
+    V = 1 << a.scale
+    s, d, w = O.rmat(a.scale, a.ef, ABCD, seed=a.seed, drop_self_loops=True, threads=os.cpu_count() or 1)
+    E = len(s)
+    sources = pick_sources(np.bincount(s, minlength=V), a.sources, a.seed)
+    L = O.refgpu()
+    if L.refgpu_upload(V, E, s, d, w) != 0:
+        return {"unavailable": "device allocation for the reference's edge list failed"}
+    del s, d, w
+    dist = np.empty(V, np.float32)
+    vis = np.empty(V, np.uint8)
+    t_bfs, t_sssp = [], []
+    try:
+        with O.quiet_stdout():
+            for src in sources.tolist():
+                tb = L.refgpu_bfs(src, vis)
+                ts = L.refgpu_sssp(src, dist)
+                if tb < 0 or ts < 0:
+                    break
+                t_bfs.append(tb)
+                t_sssp.append(ts)
+                if sum(t_bfs) + sum(t_sssp) > cap_s:
+                    break
+    finally:
+        L.refgpu_free()
+    if not t_bfs:
+        return {"unavailable": "the reference's GPU wrappers failed on this workload"}
+    total = sum(t_bfs) + sum(t_sssp)
+    return {"gteps": 2 * len(t_bfs) * E / total / 1e9, "sources": len(t_bfs), "ms_per_step_64": total / len(t_bfs) * 64e3,
+            "mean_bfs_ms": 1e3 * statistics.mean(t_bfs), "mean_sssp_ms": 1e3 * statistics.mean(t_sssp),
+            "what": "the reference's bfs_wrapper + init_distances_wrapper/bellman_ford_wrapper (its bellman_ford.cu "
+                    "and bfs.cu built unchanged for sm_100a) per source on a resident edge list; host clock around "
+                    "the wrappers as the reference times them; GTEPS = 2E x sources / total time"}
+
+
 def run_reference(a):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -512,6 +557,11 @@ def run_ours(a):
             except Exception as ex:  # the baseline is reported, never required for the GPU number
                 line["cpu_baseline"] = dict({"value": None, "unit": "GTEPS", "cores": os.cpu_count(),
                                              "kind": "reference", "sample": f"not run: {ex}"}, **host_cpu())
+        if not a.no_reference_gpu and world == 1:
+            try:
+                line["reference_gpu"] = reference_gpu_run(a)
+            except Exception as ex:  # a reported baseline, never required for the GPU number
+                line["reference_gpu"] = {"unavailable": f"not run: {ex}"}
         print(json.dumps(line), flush=True)
     g.free()
     if world > 1:

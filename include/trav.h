@@ -181,6 +181,19 @@ int trav_bellman_ford_el_f32(const int32_t *src, const int32_t *dst, const float
 int trav_bfs_el(const int32_t *src, const int32_t *dst, int32_t vertices, int64_t edges, uint8_t *visited,
                 int32_t source);
 
+/* The reachability sweep of the reference's SCC forward-backward step
+ * (bfs(), algorithm/scc/gpu/forward_backward.cu:139-170, with its kernels
+ * init_visited at :71-79 and bfs_kernel at :83-99, called forward and
+ * backward at :267-268): from the vertex *pivot, follow the edges
+ * src[e] -> dst[e] whose two ends lie in the same tree (trees[src] ==
+ * trees[dst]); visited[v] = 1 for every vertex reached, else 0 (C++ bool
+ * layout).  All arrays, pivot included, are device memory, as in the
+ * reference; the backward sweep passes dst as src.  Runs on this library's
+ * BFS kernels (the tree restriction is a vertex mask: only vertices of the
+ * pivot's tree are ever reached).  Synchronous. */
+int trav_reach_el_masked(const int32_t *src, const int32_t *dst, int32_t vertices, int64_t edges,
+                         const int32_t *pivot, const int32_t *trees, uint8_t *visited);
+
 /* ------------------------------------------------- allocation-free BFS */
 
 /* BFS levels (top-down) over a CSR the caller already holds in device
@@ -263,6 +276,12 @@ int trav_pairs_file_read(const char *path, int32_t vertices_pow, int32_t *vertic
  * b2 (32) | W3 (Ox32) | b3 (O)], row-major, tanh hidden units.  New; the
  * reference has no learned schedule. */
 int trav_mlp_set(trav_graph *g, int32_t kind, const float *params, int32_t count);
+
+/* Abstention margin of the kind's schedule network on this handle: at each
+ * decision the network keeps the plain schedule's option (Beamer's direction;
+ * delta x 1) unless its best output logit beats that option's logit by at
+ * least margin.  0 (the default) takes the plain argmax.  New. */
+int trav_mlp_set_margin(trav_graph *g, int32_t kind, float margin);
 int32_t trav_mlp_param_count(int32_t kind);
 
 /* Softmax cross-entropy loss of the kind's MLP on n samples (x: n x 10

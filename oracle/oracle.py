@@ -43,6 +43,8 @@ def lib():
         L.orc_drop_self_loops.restype = C.c_int64
         L.orc_bellman_ford.argtypes = [C.c_int32, C.c_int64, _i32p, _i32p, _f32p, C.c_int32, _f32p]
         L.orc_bellman_ford.restype = C.c_int
+        L.orc_reach_masked.argtypes = [C.c_int32, C.c_int64, _i32p, _i32p, C.c_int32, _i32p, _u8p]
+        L.orc_reach_masked.restype = C.c_int
         L.orc_dijkstra.argtypes = [C.c_int32, _i64p, _i32p, _f32p, C.c_int32, _f32p]
         L.orc_dijkstra.restype = None
         L.orc_build_csr.argtypes = [C.c_int32, C.c_int64, _i32p, _i32p, _f32p, _i64p, _i32p, _f32p]
@@ -146,6 +148,13 @@ def csr(V, src, dst, w):
     wt = np.empty(max(len(src), 1), np.float32)
     lib().orc_build_csr(V, len(src), _c(src, np.int32), _c(dst, np.int32), _c(w, np.float32), off, adj, wt)
     return off, adj, wt
+
+
+def reach_masked(V, src, dst, pivot, trees):
+    """The SCC forward-backward reachability sweep from pivot within its tree (uint8 visited)."""
+    vis = np.empty(V, np.uint8)
+    lib().orc_reach_masked(V, len(src), _c(src, np.int32), _c(dst, np.int32), int(pivot), _c(trees, np.int32), vis)
+    return vis
 
 
 def dijkstra(V, src, dst, w, source, csr_arrays=None):
@@ -299,3 +308,51 @@ def ref_rmat(V, avg, abcd=(57, 19, 19, 5), threads=1):
     w = np.empty(E, np.float32)
     ref().ref_rmat_parallel(V, avg, *abcd, threads, src, dst, w)
     return src, dst, w
+
+
+# ------------------------------------------------- the reference's GPU path
+_refgpu = None
+
+
+def refgpu_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libtrav_refgpu.so"))
+
+
+def refgpu():
+    """The reference's own bellman_ford.cu / bfs.cu built for sm_100a (oracle/_ref/libtrav_refgpu.so)."""
+    global _refgpu
+    if _refgpu is None:
+        path = os.path.join(HERE, "_ref", "libtrav_refgpu.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"reference GPU build missing: {path} (run oracle/build_refgpu.sh where the reference is)")
+        L = C.CDLL(path)
+        L.refgpu_upload.argtypes = [C.c_int, C.c_longlong, _i32p, _i32p, _f32p]
+        L.refgpu_upload.restype = C.c_int
+        L.refgpu_sssp.argtypes = [C.c_int, _f32p]
+        L.refgpu_sssp.restype = C.c_double
+        L.refgpu_bfs.argtypes = [C.c_int, _u8p]
+        L.refgpu_bfs.restype = C.c_double
+        L.refgpu_free.argtypes = []
+        L.refgpu_free.restype = None
+        _refgpu = L
+    return _refgpu
+
+
+class quiet_stdout:
+    """Send file descriptor 1 to /dev/null for a block (the reference's wrappers print with cout/printf)."""
+
+    def __enter__(self):
+        import sys
+
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        C.CDLL(None).fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+        return False

@@ -129,6 +129,30 @@ int orc_bellman_ford(int32_t V, int64_t E, const int32_t *src, const int32_t *ds
     return sweeps;
 }
 
+/* algorithm/scc/gpu/forward_backward.cu:71-99 and 139-170 (init_visited,
+ * bfs_kernel, bfs): visited = pivot only, then repeat edge sweeps marking dst
+ * when src is visited, src and dst lie in the same tree and dst is not yet
+ * visited, until a sweep marks nothing.  Returns the sweep count. */
+int orc_reach_masked(int32_t V, int64_t E, const int32_t *src, const int32_t *dst, int32_t pivot,
+                     const int32_t *trees, uint8_t *visited)
+{
+    for (int32_t i = 0; i < V; i++) visited[i] = 0;
+    visited[pivot] = 1;
+    int sweeps = 0, changes = 1;
+    while (changes) {
+        sweeps++;
+        changes = 0;
+        for (int64_t e = 0; e < E; e++) {
+            const int32_t s = src[e], t = dst[e];
+            if (visited[s] && trees[s] == trees[t] && !visited[t]) {
+                visited[t] = 1;
+                changes = 1;
+            }
+        }
+    }
+    return sweeps;
+}
+
 /* ---- binary heap keyed by float distance ---- */
 typedef struct { float key; int32_t v; } heap_item;
 

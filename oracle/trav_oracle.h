@@ -34,6 +34,11 @@ int64_t orc_drop_self_loops(int64_t E, int32_t *src, int32_t *dst, float *w);
  * over the edge list in order until a sweep changes nothing. Returns sweeps. */
 int orc_bellman_ford(int32_t V, int64_t E, const int32_t *src, const int32_t *dst, const float *w,
                      int32_t source, float *dist);
+/* The SCC forward-backward reachability sweep (algorithm/scc/gpu/
+ * forward_backward.cu:71-99, 139-170): from pivot, edges whose ends share a
+ * tree; visited[v] = 1 / 0.  Returns sweeps. */
+int orc_reach_masked(int32_t V, int64_t E, const int32_t *src, const int32_t *dst, int32_t pivot,
+                     const int32_t *trees, uint8_t *visited);
 /* Same fixpoint by label-setting (binary heap).  Equal bits to the sweep form
  * because fl(x + w) is monotone in x and >= x for w >= 0. */
 void orc_dijkstra(int32_t V, const int64_t *offsets, const int32_t *adj, const float *w,

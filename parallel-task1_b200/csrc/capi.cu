@@ -698,6 +698,17 @@ int trav_mlp_set(trav_graph *g, int32_t kind, const float *params, int32_t count
     return TRAV_OK;
 }
 
+int trav_mlp_set_margin(trav_graph *g, int32_t kind, float margin)
+{
+    if (!g) return bad("graph handle is NULL");
+    if (kind != 0 && kind != 1) return bad("kind must be 0 (BFS) or 1 (SSSP)");
+    if (!(margin >= 0.0f) || !std::isfinite(margin)) return bad("margin must be finite and >= 0");
+    TRY_CUDA(cudaSetDevice(g->device));
+    TRY_CUDA(cudaStreamSynchronize(g->st));
+    g->ws.mlp_margin[kind] = margin;
+    return TRAV_OK;
+}
+
 // ------------------------------------------------ reference-shaped entry points
 
 static __global__ void init_distances_kernel(float *d, int32_t V, int32_t s)
@@ -775,6 +786,51 @@ int trav_bfs_el(const int32_t *src, const int32_t *dst, int32_t vertices, int64_
     TRY(launch_bfs(h->g, &h->ws, 0, s_new, o, nullptr, visited, 2, h->st, nullptr, nullptr));
     TRY_CUDA(cudaStreamSynchronize(h->st));
     return check_queries(&h->ws, 1, "bfs_wrapper");
+}
+
+static __global__ void permute_color_kernel(int32_t *color_new, const int32_t *color, const int32_t *old_of_new,
+                                            int32_t V)
+{
+    for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < V; r += gridDim.x * blockDim.x)
+        color_new[r] = color[old_of_new[r]];
+}
+
+int trav_reach_el_masked(const int32_t *src, const int32_t *dst, int32_t vertices, int64_t edges,
+                         const int32_t *pivot, const int32_t *trees, uint8_t *visited)
+{
+    TRY(check_device());
+    if (!visited || !pivot || !trees || vertices < 1)
+        return bad("pivot, trees and visited must be device arrays (trees and visited of vertices >= 1 entries)");
+    if (edges < 0 || (edges > 0 && (!src || !dst))) return bad("edge arrays must be device arrays of `edges` entries");
+    if (!is_device_ptr(visited) || !is_device_ptr(pivot) || !is_device_ptr(trees) ||
+        (edges > 0 && !(is_device_ptr(src) && is_device_ptr(dst))))
+        return bad("src, dst, pivot, trees and visited must be device memory (the reference's sweep takes device arrays)");
+    if (edges >= (int64_t)INT32_MAX) {
+        set_error("graph has 2^31 or more edges; the device CSR uses int32 offsets");
+        return TRAV_ERR_OVERFLOW_INT32;
+    }
+    TRY_CUDA(cudaDeviceSynchronize());
+    int32_t p = 0;
+    TRY_CUDA(cudaMemcpy(&p, pivot, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (p < 0 || p >= vertices) return bad("the pivot vertex lies outside [0, V)");
+    int32_t want = 0;
+    TRY_CUDA(cudaMemcpy(&want, trees + p, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    trav_graph *h = nullptr;
+    TRY(new_handle(&h));
+    std::unique_ptr<trav_graph, void (*)(trav_graph *)> guard(h, destroy);
+    TRY(build_graph_device(vertices, edges, src, dst, nullptr, h->st, &h->g));
+    TRY(workspace_ensure(&h->ws, h->g, 1, h->st));
+    DevTmp<int32_t> color;
+    TRY_CUDA(dev_malloc(&color.p, sizeof(int32_t) * (size_t)vertices));
+    permute_color_kernel<<<(vertices + 255) / 256 < 4096 ? (vertices + 255) / 256 : 4096, 256, 0, h->st>>>(
+        color.p, trees, h->g.old_of_new, vertices);
+    TRY_CUDA(cudaGetLastError());
+    trav_bfs_opts o{TRAV_SCHEDULE_PLAIN, 15.0f, 18.0f, -1};
+    int32_t p_new = 0;
+    TRY_CUDA(cudaMemcpy(&p_new, h->g.new_of_old + p, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    TRY(launch_bfs(h->g, &h->ws, 0, p_new, o, nullptr, visited, 2, h->st, nullptr, nullptr, color.p, want));
+    TRY_CUDA(cudaStreamSynchronize(h->st));
+    return check_queries(&h->ws, 1, "trav_reach_el_masked");
 }
 
 // ----------------------------------------------------------- graph files

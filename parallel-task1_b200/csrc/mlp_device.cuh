@@ -100,8 +100,12 @@ __host__ __device__ inline float sssp_width_scale(int option) { return (float)(1
 // (O independent shuffle chains).  All 32 lanes must call; lane 0's argmax
 // (lowest index on ties) is returned in every lane.  The summation order is
 // fixed, so every CTA computes the same decision.
+//
+// Abstention: with margin > 0 the network keeps the plain schedule's option
+// `plain` unless its best logit beats plain's by at least margin, so a network
+// that is unsure (or wrong by little) does not override its fallback.
 template <int O>
-__device__ inline int mlp_argmax_warp(const float *p, const Feat &f)
+__device__ inline int mlp_argmax_warp(const float *p, const Feat &f, int plain = 0, float margin = 0.0f)
 {
     const int j = threadIdx.x & 31;
     const float *W1 = p, *b1 = W1 + kHidden * kFeat, *W2 = b1 + kHidden, *b2 = W2 + kHidden * kHidden;
@@ -123,15 +127,17 @@ __device__ inline int mlp_argmax_warp(const float *p, const Feat &f)
         for (int o = 0; o < O; o++) t[o] += __shfl_xor_sync(0xffffffffu, t[o], s);
     }
     int best = 0;
-    float bestv = -INFINITY;
+    float bestv = -INFINITY, plainv = -INFINITY;
 #pragma unroll
     for (int o = 0; o < O; o++) {
         const float v = t[o] + b3[o];
+        if (o == plain) plainv = v;
         if (v > bestv) {
             bestv = v;
             best = o;
         }
     }
+    if (margin > 0.0f && bestv - plainv < margin) best = plain;
     // the butterfly sums may round differently per lane: lane 0 decides
     return __shfl_sync(0xffffffffu, best, 0);
 }

@@ -23,12 +23,18 @@ constexpr int kMaxDec = 1024;     // schedule decisions recorded per query
 constexpr int kDecFeat = 10;      // features per decision (the schedule MLP's input width)
 constexpr int kSlots = 4;         // ring of per-phase counter slots
 constexpr unsigned long long kDefaultTimeoutNs = 10ull * 1000000000ull;  // grid-barrier wait limit (10 s)
-// Row-class flags in the low bits of an SSSP distance word (dist_bits << 32 |
-// round << kClsBits | flags): which parts of the vertex's out-row are non-empty
-// and which are longer than kSmallDeg.  They depend only on the graph and
-// delta, so the 64-bit atomicMin that lowers a distance keeps them.
+// Row-class flags of a vertex for SSSP (one byte per vertex, written at a
+// query's initialisation): which parts of its out-row are non-empty and which
+// are longer than the warp-tile threshold.  They depend only on the graph and
+// delta.  An SSSP distance word is dist_bits << 32 | round << kClsBits; its
+// low kClsBits bits stay zero.
 constexpr unsigned kClsLight = 1, kClsLightBig = 2, kClsHeavy = 4, kClsHeavyBig = 8;
 constexpr unsigned kClsBits = 4, kClsMask = (1u << kClsBits) - 1u;
+// Distance filter of SSSP: qd[v] >= (bits of v's distance) >> kQdShift at all
+// times (0xFFFF while v is unreached), a 16-bit upper bound on the distance's
+// quantised bits.  A candidate whose quantised bits exceed it cannot lower v.
+constexpr unsigned kQdShift = 15;
+constexpr unsigned short kQdUnreached = 0xFFFFu;
 constexpr int kMaxRounds = (1 << (32 - kClsBits)) - 1;  // round ids of one SSSP launch must fit the stamp
 
 // Device status codes written to Ctl::err.
@@ -105,8 +111,10 @@ struct Workspace {
     int32_t V = 0;
     int64_t chunk_cap = 0;
     // V 64-bit words: BFS levels (int32, the first V words) or SSSP distance
-    // words (float bits << 32 | round << kClsBits | row-class flags)
+    // words (float bits << 32 | round << kClsBits)
     unsigned int *value = nullptr;
+    unsigned short *qd = nullptr;      // V: SSSP distance filter (see kQdShift)
+    unsigned char *rcls = nullptr;     // V: SSSP row-class flags
     unsigned int *visited = nullptr;   // W words
     unsigned int *front[2] = {nullptr, nullptr};  // W words each
     int32_t *queue[2] = {nullptr, nullptr};       // V each
@@ -124,6 +132,7 @@ struct Workspace {
     int small_deg = kSmallDeg;         // expansion thresholds of the launches (see TravArgs)
     int item = kItem;
     int max_steps = 0;                 // step budget of a query; 0 = the default (see launch_bfs / launch_sssp)
+    float mlp_margin[2] = {0.0f, 0.0f};  // abstention margins of the BFS / SSSP networks
     unsigned long long timeout_ns = 0;  // bounded wait of a grid barrier; 0 = kDefaultTimeoutNs
 };
 
@@ -143,6 +152,8 @@ struct TravArgs {
     // workspace
     unsigned int *value;        // BFS levels
     unsigned long long *dist;   // SSSP distance words (same memory as value)
+    unsigned short *qd;         // SSSP distance filter (see kQdShift)
+    unsigned char *rcls;        // SSSP row-class flags of each vertex
     unsigned int *visited;
     unsigned int *front0, *front1;
     int32_t *q0, *q1;
@@ -160,6 +171,10 @@ struct TravArgs {
     // BFS options
     float alpha, beta;
     int32_t force_dir;
+    // BFS vertex mask (new ids; nullptr = none): only vertices v with
+    // color[v] == color_want are reached (the SCC sweeps' tree restriction)
+    const int32_t *color;
+    int32_t color_want;
     // SSSP options
     float delta;           // +inf = Bellman-Ford
     float mean_w;          // mean edge weight of the graph
@@ -167,8 +182,10 @@ struct TravArgs {
     // output (original ids); nullptr = leave results in `value`
     void *out;
     int32_t out_kind;      // 0 = int32 levels, 1 = float distances, 2 = uint8 reached flags
-    // learned schedule (nullptr = plain)
+    // learned schedule (nullptr = plain); mlp_margin > 0: the network keeps
+    // the plain option unless its best logit beats it by that much
     const float *mlp;
+    float mlp_margin;
     // forced decisions: plan[i] (< 255) overrides decision i of the query
     const unsigned char *plan;
     int32_t plan_len;
@@ -186,6 +203,7 @@ struct BatchQuery {
     const float *out_w, *in_w;
     const int32_t *nlight;  // SSSP light-prefix lengths for delta; nullptr = Bellman-Ford
     const float *mlp;       // schedule network; nullptr = plain schedule
+    float mlp_margin;       // logit margin the network needs to leave the plain option
     void *out;              // results in original ids: int32 levels (BFS) or float distances (SSSP)
     int64_t E;
     int32_t V;
@@ -199,6 +217,8 @@ struct BatchQuery {
 // Scratch of one team of a batch launch, sized for the batch's largest graph.
 struct TeamWs {
     unsigned int *value;  // 2 * Vmax words
+    unsigned short *qd;   // Vmax
+    unsigned char *rcls;  // Vmax
     unsigned int *visited, *front0, *front1;
     int32_t *q0, *q1, *far0, *far1, *hq0, *hq1;
     int2 *chunks0, *chunks1, *hch0, *hch1;
@@ -255,8 +275,10 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
 void workspace_free(Workspace *ws);
 // Enqueue one query on st using control block ws->ctl[q] (no host sync).
 // ev0/ev1 (optional) are recorded around the launch.
+// color (new ids, may be nullptr): reach only vertices with color[v] == color_want.
 int launch_bfs(const DevGraph &g, Workspace *ws, int q, int32_t source_new, const trav_bfs_opts &o,
-               const float *mlp, void *out, int out_kind, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1);
+               const float *mlp, void *out, int out_kind, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
+               const int32_t *color = nullptr, int32_t color_want = 0);
 int launch_sssp(const DevGraph &g, Workspace *ws, int q, int32_t source_new, float delta, const float *mlp,
                 void *out, int out_kind, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1);
 // After the stream finished: turn the device status of queries [0, n) into a return code.

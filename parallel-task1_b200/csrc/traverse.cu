@@ -94,6 +94,22 @@ __device__ __forceinline__ unsigned long long ld_gather(const unsigned long long
 #endif
 }
 
+// gather of a mutable 16-bit filter entry at L2, evict-last: the filter array
+// (2 bytes per vertex) is meant to stay L2-resident while the 8-byte distance
+// words it screens are touched only by the atomics of candidates
+__device__ __forceinline__ unsigned ld_gather_u16(const unsigned short *p)
+{
+#if TRAV_L2HINT
+    unsigned short v;
+    asm volatile("ld.global.cg.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(l2_policy_evict_last()));
+    return v;
+#else
+    return __ldcg(p);
+#endif
+}
+
+__device__ __forceinline__ unsigned short qd_of(float d) { return (unsigned short)(__float_as_uint(d) >> kQdShift); }
+
 __device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned *p)
 {
     unsigned v;
@@ -513,7 +529,6 @@ constexpr int kWDefer = 32 + 32 * kBatchSssp;
 struct DeferStage {
     int v[kWDefer];
     float d[kWDefer];
-    unsigned cls[kWDefer];
 };
 
 struct CtaCounters {
@@ -848,9 +863,9 @@ struct BfsPush {
     }
 };
 
-// SSSP distance word: float bits in the high half, the round stamp and the
-// row-class flags in the low half.  Distances are >= +0, so the unsigned order
-// of the words is the order of the distances (ties broken by the stamp).
+// SSSP distance word: float bits in the high half, the round stamp in the low
+// half.  Distances are >= +0, so the unsigned order of the words is the order
+// of the distances (ties broken by the stamp).
 __device__ __forceinline__ float dist_of(unsigned long long x) { return __uint_as_float((unsigned)(x >> 32)); }
 
 __device__ __forceinline__ unsigned long long pack_dist(float d, unsigned low)
@@ -859,13 +874,13 @@ __device__ __forceinline__ unsigned long long pack_dist(float d, unsigned low)
 }
 
 // SSSP relaxation.  A distance is one 64-bit word: the float bits, then the
-// id of the round that last lowered it, then the row-class flags:
-//     dist_bits << 32 | round << 4 | flags.
-// The atomicMin that lowers a distance writes the current round and keeps the
-// flags, and its return value tells the thread both whether it improved the
-// vertex and when the vertex was last improved -- which is all the push needs
-// to decide, without another atomic, whether the vertex is already in the
-// buffer it belongs to:
+// id of the round that last lowered it:
+//     dist_bits << 32 | round << 4.
+// The atomicMin that lowers a distance writes the current round, and its
+// return value tells the thread both whether it improved the vertex and when
+// the vertex was last improved -- which, with the vertex's row-class byte, is
+// all the push needs to decide, without another atomic, whether the vertex is
+// already in the buffer it belongs to:
 //   - next frontier (light prefix, this round only): already there when the
 //     old word is from this round and below the bound;
 //   - heavy list (since h_start): already there when the old word is from a
@@ -944,33 +959,37 @@ struct SsspVisit {
         }
     }
 
-    // An edge whose candidate beats the gathered distance is not relaxed at
-    // once: (v, candidate, row class) goes to the warp's DeferStage, and the
-    // atomicMins run 32 at a time (drain).  A batch then waits on its edge
-    // loads and its gathers only; the wait for an atomic's return -- which
-    // every batch used to pay, since almost every batch of 32 * kBatch edges
-    // has an improving lane -- comes once per 32 candidates.  The candidates
-    // are relaxed within the same phase, and the push decision reads only the
-    // atomic's return value, so the order of the atomics changes nothing.
+    // An edge is screened by the target's 16-bit distance filter, not by its
+    // 8-byte distance word: qd[v] is an upper bound on the quantised bits of
+    // v's distance, so a candidate whose quantised bits exceed it cannot lower
+    // v and is dropped.  The filter array (2 bytes per vertex) stays in L2,
+    // where the distance words of a batch's concurrent queries do not fit.
+    // Any other candidate is not relaxed at once: (v, candidate) goes to the
+    // warp's DeferStage, and the atomicMins run 32 at a time (drain).  A batch
+    // then waits on its edge loads and its filter gathers only; the wait for
+    // an atomic's return comes once per 32 candidates.  The candidates are
+    // relaxed within the same phase, and the push decision reads only the
+    // atomic's return value, so the order of the atomics changes nothing; a
+    // candidate the filter lets through that does not improve v is refused by
+    // its atomicMin.
     __device__ __forceinline__ void visit_loaded(const float (&du)[kBatch], const int (&v)[kBatch],
                                                  const float (&w)[kBatch], const bool (&ok)[kBatch], Pusher &p) const
     {
         float nd[kBatch];
-        unsigned long long cur[kBatch];
+        unsigned qv[kBatch];
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) qv[j] = ok[j] ? ld_gather_u16(&a->qd[v[j]]) : 0u;
 #pragma unroll
         for (int j = 0; j < kBatch; j++) nd[j] = ok[j] ? __fadd_rn(du[j], w[j]) : 0.0f;  // one rounded add, as sssp.hpp:56
-#pragma unroll
-        for (int j = 0; j < kBatch; j++) cur[j] = ok[j] ? ld_gather(&a->dist[v[j]]) : 0ull;
         DeferStage *d = p.d;
 #pragma unroll
         for (int j = 0; j < kBatch; j++) {
-            const bool cand = ok[j] && nd[j] < dist_of(cur[j]);
+            const bool cand = ok[j] && (unsigned)qd_of(nd[j]) <= qv[j];
             const unsigned m = __ballot_sync(kFull, cand);
             if (cand) {
                 const unsigned i = p.ndef + __popc(m & lanemask_lt());
                 d->v[i] = v[j];
                 d->d[i] = nd[j];
-                d->cls[i] = (unsigned)cur[j] & kClsMask;
             }
             p.ndef += __popc(m);
         }
@@ -993,22 +1012,25 @@ struct SsspVisit {
         const bool ok = lane < n;
         int v = 0;
         float nd = 0.0f;
-        unsigned cls = 0;
         if (ok) {
             v = d->v[base + lane];
             nd = d->d[base + lane];
-            if constexpr (!kPull) cls = d->cls[base + lane];
         }
         __syncwarp();  // the entries are read before later batches overwrite them
-        if constexpr (kPull) {
-            if (ok) cls = row_class(*a, v);  // the owner's flags (a pull stages no gathered word of it)
-        }
         p.ndef = base;
         bool light = false, heavy = false, far = false;
+        unsigned cls = 0;
         if (ok) {
-            const unsigned long long old = atomicMin(&a->dist[v], pack_dist(nd, round << kClsBits | cls));
+            // written at this query's initialisation (by other CTAs, and a team
+            // rewrites it per query): read at L2, not through the read-only
+            // path; independent of the atomic, so both round trips overlap
+            cls = __ldcg(&a->rcls[v]);
+            const unsigned long long old = atomicMin(&a->dist[v], pack_dist(nd, round << kClsBits));
             const float od = dist_of(old);
             if (nd < od) {
+                // nd is now an upper bound of v's distance; a racing store of a
+                // larger bound only lets more candidates through
+                a->qd[v] = qd_of(nd);
                 const unsigned orr = (unsigned)old >> kClsBits;
                 if (nd < thr) {
                     const bool seen_below = od < thr;
@@ -1080,7 +1102,18 @@ __device__ __forceinline__ int bfs_query(const TravArgs &a, QueryShared &sh, int
     load_mlp(a, sh, mlp_param_count(kBfsOut));
     init_counters(cc);
     for (int v = gtid; v < a.V; v += nth) reinterpret_cast<int *>(a.value)[v] = v == s ? 0 : -1;
-    for (int w = gtid; w < a.W; w += nth) a.visited[w] = w == (s >> 5) ? 1u << (s & 31) : 0u;
+    if (!a.color) {
+        for (int w = gtid; w < a.W; w += nth) a.visited[w] = w == (s >> 5) ? 1u << (s & 31) : 0u;
+    } else {
+        // vertex mask: vertices of another color start out visited, so no
+        // step (top-down or bottom-up) ever reaches them; their levels stay -1
+        for (unsigned w = gwarp; w < (unsigned)a.W; w += nwarps) {
+            const int v = (int)(w * 32 + lane_id());
+            const bool pre = v < a.V && (v == s || __ldg(&a.color[v]) != a.color_want);
+            const unsigned m = __ballot_sync(kFull, pre);
+            if (lane_id() == 0) a.visited[w] = m;
+        }
+    }
     unsigned nq, nch;
     seed_part(a, s, __ldg(&a.out_off[s]), __ldg(&a.out_off[s + 1]), a.q0, a.chunks0, nq, nch);
     clear_ahead(a, ph);
@@ -1107,7 +1140,7 @@ __device__ __forceinline__ int bfs_query(const TravArgs &a, QueryShared &sh, int
             const Feat f = bfs_features(L, nf, mf, mu, nf_prev, a.V, a.E, prev_dir, plain);
             int d = plain;
             if (a.force_dir >= 0) d = (L == 0) ? 0 : a.force_dir;
-            else if (a.mlp) d = mlp_argmax_warp<kBfsOut>(sh.mlp, f);
+            else if (a.mlp) d = mlp_argmax_warp<kBfsOut>(sh.mlp, f, plain, a.mlp_margin);
             const int forced = planned(a, L);
             if (forced >= 0) d = forced;
             log_decision(ctl, lg, f, d, 0.0f, 0.0f);
@@ -1290,8 +1323,9 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
     if (a.source >= 0) {
         const int s = a.source;
         for (int v = gtid; v < a.V; v += nth) {
-            const unsigned cls = row_class(a, v);
-            a.dist[v] = pack_dist(v == s ? 0.0f : FLT_MAX, cls);
+            a.rcls[v] = (unsigned char)row_class(a, v);
+            a.dist[v] = pack_dist(v == s ? 0.0f : FLT_MAX, 0u);
+            a.qd[v] = v == s ? (unsigned short)0 : kQdUnreached;
         }
         const int2 lp = row_part(a, s, lpart);
         seed_part(a, s, lp.x, lp.y, a.q0, a.chunks0, nq, nch);
@@ -1319,7 +1353,9 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
             if (v < a.V) {
                 bits = __ldg(&a.init_bits[v]);
                 cls = row_class(a, v);
-                a.dist[v] = (static_cast<unsigned long long>(bits) << 32) | cls;
+                a.rcls[v] = (unsigned char)cls;
+                a.dist[v] = static_cast<unsigned long long>(bits) << 32;
+                a.qd[v] = bits < kFltMaxBits ? (unsigned short)(bits >> kQdShift) : kQdUnreached;
             }
             const bool act = bits < kFltMaxBits && (cls & kClsLight);
             push(p, 0, act, v, cls & kClsLightBig ? big_len : 1u);
@@ -1450,7 +1486,7 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
                 const Feat f = sssp_features(steps, far_len, __int_as_float(min_far), thr, a.delta, a.V, a.E, buckets, a.mean_w,
                                              a.max_deg);
                 int o = 0;
-                if (a.mlp) o = mlp_argmax_warp<kSsspOut>(sh.mlp, f);
+                if (a.mlp) o = mlp_argmax_warp<kSsspOut>(sh.mlp, f, 0, a.mlp_margin);
                 const int forced = planned(a, buckets - 1);
                 if (forced >= 0) o = forced;
                 const float width = a.delta * sssp_width_scale(o);
@@ -1483,14 +1519,14 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
                 const bool valid = i < far_len;
                 const int v = valid ? fp[i] : 0;
                 const unsigned long long dv = valid ? __ldcg(&a.dist[v]) : 0ull;
+                const unsigned cls = valid ? __ldcg(&a.rcls[v]) : 0u;
                 const float d = dist_of(dv);
-                const unsigned cls = (unsigned)dv;
                 const bool in_bucket = valid && d >= told && d < thr;
                 // the pile holds each vertex once (see SsspPush), so every entry is pushed on
                 const bool light = in_bucket && (cls & kClsLight);
                 const bool heavy = in_bucket && (cls & kClsHeavy);
                 const bool keep = valid && d >= thr;
-                if (in_bucket || keep) atomicMax(&a.dist[v], pack_dist(d, round << kClsBits | (cls & kClsMask)));
+                if (in_bucket || keep) atomicMax(&a.dist[v], pack_dist(d, round << kClsBits));
                 push(p, 0, light, v, cls & kClsLightBig ? big_len : 1u);
                 push(p, 1, heavy, v, cls & kClsHeavyBig ? big_len : 1u);
                 push_far(p, keep, v, keep ? 0x7fffffff - __float_as_int(d) : 0);
@@ -1574,6 +1610,8 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) batch_persistent
         a.E = q.E;
         a.value = w.value;
         a.dist = reinterpret_cast<unsigned long long *>(w.value);
+        a.qd = w.qd;
+        a.rcls = w.rcls;
         a.visited = w.visited;
         a.front0 = w.front0;
         a.front1 = w.front1;
@@ -1592,6 +1630,7 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) batch_persistent
         a.source = q.source;
         a.out = q.out;
         a.mlp = q.mlp;
+        a.mlp_margin = q.mlp_margin;
         a.plan = nullptr;
         a.plan_len = 0;
         a.small_deg = b.small_deg;
@@ -1844,6 +1883,8 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
     ws->V = g.V;
     ws->chunk_cap = V + g.E / kMinItem + 1;
     TRY_CUDA(dev_malloc(&ws->value, sizeof(unsigned long long) * V));
+    TRY_CUDA(dev_malloc(&ws->qd, sizeof(unsigned short) * V));
+    TRY_CUDA(dev_malloc(&ws->rcls, sizeof(unsigned char) * V));
 
     TRY_CUDA(dev_malloc(&ws->visited, sizeof(unsigned) * W));
     TRY_CUDA(dev_malloc(&ws->front[0], sizeof(unsigned) * W));
@@ -1868,6 +1909,8 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
 void workspace_free(Workspace *ws)
 {
     cudaFree(ws->value);
+    cudaFree(ws->qd);
+    cudaFree(ws->rcls);
     cudaFree(ws->visited);
     cudaFree(ws->front[0]);
     cudaFree(ws->front[1]);
@@ -1903,6 +1946,8 @@ static TravArgs make_args(const DevGraph &g, Workspace *ws)
     a.E = g.E;
     a.value = ws->value;
     a.dist = reinterpret_cast<unsigned long long *>(ws->value);
+    a.qd = ws->qd;
+    a.rcls = ws->rcls;
     a.visited = ws->visited;
     a.front0 = ws->front[0];
     a.front1 = ws->front[1];
@@ -1929,9 +1974,12 @@ static TravArgs make_args(const DevGraph &g, Workspace *ws)
 }
 
 int launch_bfs(const DevGraph &g, Workspace *ws, int q, int32_t source_new, const trav_bfs_opts &o,
-               const float *mlp, void *out, int out_kind, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1)
+               const float *mlp, void *out, int out_kind, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
+               const int32_t *color, int32_t color_want)
 {
     TravArgs a = make_args(g, ws);
+    a.color = color;
+    a.color_want = color_want;
     a.ctl = ws->ctl + q;
     a.source = source_new;
     a.max_steps = g.V + 1;
@@ -1943,6 +1991,7 @@ int launch_bfs(const DevGraph &g, Workspace *ws, int q, int32_t source_new, cons
     a.out = out;
     a.out_kind = out_kind;
     a.mlp = mlp;
+    a.mlp_margin = ws->mlp_margin[0];
     a.plan = ws->plan[0];
     a.plan_len = ws->plan_len[0];
     return enqueue_persistent(0, a, ws->grid[0], st, ev0, ev1);
@@ -1974,6 +2023,7 @@ int launch_sssp(const DevGraph &g, Workspace *ws, int q, int32_t source_new, flo
     a.out = out;
     a.out_kind = out_kind;
     a.mlp = mlp;
+    a.mlp_margin = ws->mlp_margin[1];
     a.plan = ws->plan[1];
     a.plan_len = ws->plan_len[1];
     return enqueue_persistent(1, a, ws->grid[1], st, ev0, ev1);

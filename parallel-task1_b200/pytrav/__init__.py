@@ -52,7 +52,8 @@ EXPORTS = [
     "trav_last_decisions", "trav_set_grid", "trav_batch_create", "trav_batch_free", "trav_batch_run",
     "trav_batch_autotune", "trav_batch_set_shape", "trav_batch_get_shape", "trav_graph_set_capture",
     "trav_el_optimize", "trav_el_gpu_transactions", "trav_adj_file_read", "trav_adj_file_write",
-    "trav_pairs_file_read", "trav_set_limits", "trav_inject_alloc_failure",
+    "trav_pairs_file_read", "trav_set_limits", "trav_inject_alloc_failure", "trav_reach_el_masked",
+    "trav_mlp_set_margin",
 ]
 
 
@@ -113,12 +114,14 @@ def lib():
         L.trav_init_distances_f32.argtypes = [vp, i32, i32]
         L.trav_bellman_ford_el_f32.argtypes = [vp, vp, vp, i32, i64, i32, vp]
         L.trav_bfs_el.argtypes = [vp, vp, i32, i64, vp, i32]
+        L.trav_reach_el_masked.argtypes = [vp, vp, i32, i64, vp, vp, vp]
         L.trav_el_file_read.argtypes = [C.c_char_p, i32, C.POINTER(i32), C.POINTER(i64), C.POINTER(i32), vp, vp, vp]
         L.trav_el_file_write.argtypes = [C.c_char_p, i32, i32, i64, vp, vp, vp]
         L.trav_adj_file_read.argtypes = [C.c_char_p, C.POINTER(i32), C.POINTER(i64), C.POINTER(i32)] + [vp] * 5
         L.trav_adj_file_write.argtypes = [C.c_char_p, i32, i32, i64] + [vp] * 5
         L.trav_pairs_file_read.argtypes = [C.c_char_p, i32, C.POINTER(i32), C.POINTER(i64), vp, vp, vp]
         L.trav_mlp_set.argtypes = [vp, i32, vp, i32]
+        L.trav_mlp_set_margin.argtypes = [vp, i32, f32]
         L.trav_set_grid.argtypes = [vp, i32, i32, C.POINTER(i32)]
         L.trav_graph_set_capture.argtypes = [vp, i32]
         L.trav_el_optimize.argtypes = [vp, vp, vp, i32, i64, i32, i32, C.POINTER(i64)]
@@ -326,6 +329,10 @@ class Graph:
     def set_mlp(self, kind: int, params):
         p = np.ascontiguousarray(params, np.float32)
         _check(lib().trav_mlp_set(self._h, kind, p.ctypes.data, len(p)))
+
+    def set_mlp_margin(self, kind: int, margin: float):
+        """Logit margin the kind's network needs to leave the plain option (0 = plain argmax)."""
+        _check(lib().trav_mlp_set_margin(self._h, kind, float(margin)))
 
     def out_degrees(self):
         """Out-degree of every vertex in the caller's ids."""

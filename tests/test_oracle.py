@@ -219,3 +219,27 @@ def test_el_optimize_live_reference_small_segments():
         assert n == len(ms)
         assert sorted(zip(ms.tolist(), md.tolist(), mw.tolist())) == sorted(zip(rs.tolist(), rd.tolist(), rw.tolist()))
         g.free()
+
+
+def test_masked_reach_restatement_is_reachability_inside_the_pivots_tree():
+    """orc_reach_masked (the SCC sweep) equals a queue BFS over the edges whose ends share the pivot's tree."""
+    import collections
+
+    V = 1 << 9
+    s, d, _ = O.rmat(9, 8, seed=6, drop_self_loops=False)
+    trees = np.random.default_rng(1).integers(0, 3, V).astype(np.int32)
+    adj = collections.defaultdict(list)
+    for a, b in zip(s.tolist(), d.tolist()):
+        if trees[a] == trees[b]:
+            adj[a].append(b)
+    for pivot in (0, int(np.bincount(s, minlength=V).argmax())):
+        want = np.zeros(V, np.uint8)
+        want[pivot] = 1
+        q = collections.deque([pivot])
+        while q:
+            u = q.popleft()
+            for v in adj[u]:
+                if not want[v]:
+                    want[v] = 1
+                    q.append(v)
+        assert np.array_equal(O.reach_masked(V, s, d, pivot, trees), want)
