@@ -47,8 +47,7 @@ struct trav_batch {
     BatchQuery *d_q = nullptr;
     int q_cap = 0;
     unsigned *d_next = nullptr;
-    // light-prefix lengths per (graph, delta)
-    std::map<std::pair<int, float>, int32_t *> nlight;
+    std::map<std::pair<int, float>, LightRows> light;  // light rows per (graph, delta)
     trav_batch_shape shape{16, kSmallDeg, kItem};
 };
 
@@ -180,17 +179,16 @@ int build_queries(trav_batch *b, const trav_query *qs, int32_t n, std::vector<Ba
         d.mlp_margin = g->ws.mlp_margin[q.kind];
         d.delta = INFINITY;
         d.nlight = nullptr;
+        d.loff = nullptr;
+        d.ledge = nullptr;
         if (q.kind == 1 && finite_delta(q.delta)) {
             d.delta = q.delta;
-            auto key = std::make_pair(q.graph, q.delta);
-            auto it = b->nlight.find(key);
-            if (it == b->nlight.end()) {
-                int32_t *p = nullptr;
-                TRY_CUDA(dev_malloc(&p, sizeof(int32_t) * (size_t)std::max<int32_t>(g->g.V, 1)));
-                it = b->nlight.emplace(key, p).first;
-                TRY(count_light(g->g, q.delta, p, b->st));
-            }
-            d.nlight = it->second;
+            // light rows once per (graph, delta) for the batch's lifetime
+            LightRows &lr = b->light[std::make_pair(q.graph, q.delta)];
+            TRY(light_rows_build(g->g, q.delta, &lr, b->st));
+            d.nlight = lr.nlight;
+            d.loff = lr.loff;
+            d.ledge = lr.ledge;
         }
         out->push_back(d);
     }
@@ -328,7 +326,7 @@ void trav_batch_free(trav_batch *b)
     cudaFree(b->ctl);
     cudaFree(b->d_q);
     cudaFree(b->d_next);
-    for (auto &kv : b->nlight) cudaFree(kv.second);
+    for (auto &kv : b->light) light_rows_free(&kv.second);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->st) cudaStreamDestroy(b->st);

@@ -177,6 +177,9 @@ std::vector<unsigned char> capture_key(const trav_graph *g, int kind, const int3
     put(k, g->ws.plan[kind]);
     put(k, g->ws.plan_len[kind]);
     put(k, g->ws.max_steps);
+    put(k, g->ws.light.nlight);
+    put(k, g->ws.light.loff);
+    put(k, g->ws.light.ledge);
     put(k, g->ws.timeout_ns);
     put(k, g->st);
     put(k, g->ws.ctl);
@@ -225,12 +228,15 @@ int run_batch(trav_graph *g, int kind, const int32_t *sources, int32_t n, const 
     };
     if (g->capture && mem == TRAV_MEM_DEVICE) {
         trav_graph::Captured &c = g->cap[kind];
+        // the light rows of delta are built before the capture (it allocates
+        // and synchronises); the graph bakes in their addresses, which are part
+        // of the key, so a rebuild for another delta records a new graph
+        if (kind == 1 && delta > 0.0f && std::isfinite(delta)) TRY(light_rows_build(g->g, delta, &g->ws.light, g->st));
         std::vector<unsigned char> key = capture_key(g, kind, sources, n, bo, delta, mlp, out);
         if (!c.exec || c.key != key) {
             if (c.exec) cudaGraphExecDestroy(c.exec);
             c.exec = nullptr;
             c.key.clear();
-            if (kind == 1) g->ws.nlight_delta = -1.0f;  // the graph must count the light prefixes itself
             TRY_CUDA(cudaStreamBeginCapture(g->st, cudaStreamCaptureModeThreadLocal));
             const int rc = enqueue();
             cudaGraph_t graph = nullptr;
@@ -246,8 +252,6 @@ int run_batch(trav_graph *g, int kind, const int32_t *sources, int32_t n, const 
             c.key = std::move(key);
         }
         TRY_CUDA(cudaGraphLaunch(c.exec, g->st));
-        // the graph recounts the light prefixes for its own delta
-        if (kind == 1) g->ws.nlight_delta = -1.0f;
     } else {
         TRY(enqueue());
     }

@@ -106,6 +106,17 @@ struct DevGraph {
     int32_t *old_of_new = nullptr;  // V
 };
 
+// Light rows of a graph for one delta: the light-prefix length of every row
+// and, when the light rows are packed (TRAV_LIGHT_ROWS), the prefixes
+// themselves in a CSR of their own (see TravArgs::loff / ledge).
+struct LightRows {
+    float delta = -1.0f;          // < 0: not built
+    int32_t *nlight = nullptr;    // V
+    int32_t *loff = nullptr;      // V + 1; nullptr when the prefixes are not packed
+    int2 *ledge = nullptr;        // loff[V] edges {target, weight bits}
+    int64_t edges = 0;            // light edges of the graph for delta
+};
+
 // Per-handle traversal workspace (scratch memory of the persistent kernels).
 struct Workspace {
     int32_t V = 0;
@@ -121,8 +132,7 @@ struct Workspace {
     int32_t *far[2] = {nullptr, nullptr};         // V each
     int32_t *hq[2] = {nullptr, nullptr};  // SSSP heavy lists (short heavy parts), V each
     int2 *hchunks[2] = {nullptr, nullptr};  // SSSP heavy lists (chunk items), chunk_cap each
-    int32_t *nlight = nullptr;         // V: out-edges lighter than nlight_delta (rows are sorted by weight)
-    float nlight_delta = -1.0f;        // delta nlight was counted for (< 0: none)
+    LightRows light;                   // light rows for the last finite delta (rows are sorted by weight)
     int2 *chunks[2] = {nullptr, nullptr};  // chunk_cap items each (current / next frontier)
     Ctl *ctl = nullptr;                // ctl_cap control blocks: one per query of a batch
     int ctl_cap = 0;
@@ -161,6 +171,10 @@ struct TravArgs {
     int32_t *hq0, *hq1;       // SSSP heavy lists
     int2 *hch0, *hch1;
     const int32_t *__restrict__ nlight;  // light-prefix length per vertex; nullptr = every edge is light
+    // light rows (nullptr = none): the light prefixes packed by themselves,
+    // row v = ledge[loff[v] .. loff[v+1]), each edge {target, weight bits}
+    const int32_t *__restrict__ loff;
+    const int2 *__restrict__ ledge;
     int2 *chunks;          // chunk items (two-phase expansion)
     int2 *chunks0, *chunks1;  // chunk items of the current / next frontier (one-phase expansion)
     Ctl *ctl;
@@ -202,6 +216,8 @@ struct BatchQuery {
     const int32_t *out_off, *out_adj, *in_off, *in_adj, *new_of_old;
     const float *out_w, *in_w;
     const int32_t *nlight;  // SSSP light-prefix lengths for delta; nullptr = Bellman-Ford
+    const int32_t *loff;    // packed light rows (nullptr = none)
+    const int2 *ledge;
     const float *mlp;       // schedule network; nullptr = plain schedule
     float mlp_margin;       // logit margin the network needs to leave the plain option
     void *out;              // results in original ids: int32 levels (BFS) or float distances (SSSP)
@@ -286,6 +302,9 @@ int check_queries(Workspace *ws, int n, const char *what);
 int check_ctls(const Ctl *ctl, int n, const char *what);  // the same for n device control blocks
 // Light-prefix length of every row of g for delta (rows are sorted by weight).
 int count_light(const DevGraph &g, float delta, int32_t *nlight, cudaStream_t st);
+// Build (or rebuild for a new delta) the light rows of g; no-op when lr already holds delta.
+int light_rows_build(const DevGraph &g, float delta, LightRows *lr, cudaStream_t st);
+void light_rows_free(LightRows *lr);
 int query_bytes(const DevGraph &g, Workspace *ws, int q, int kind, int64_t *bytes, int64_t *reached,
                 int64_t *reached_edges, cudaStream_t st);
 int persistent_grid_size(int kind);  // kind 2 = the batch kernel

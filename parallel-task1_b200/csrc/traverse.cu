@@ -13,6 +13,8 @@
 //   level_init_kernel / bfs_kernel / bfs_wrapper algorithm/bfs/gpu/bfs.cu:12-81
 //   cpu_bellman_ford relaxation                 algorithm/sssp/sssp.hpp:47-61
 //   cpu_parallel_bfs level loop                 algorithm/bfs/bfs.hpp:150-206
+#include <cub/device/device_scan.cuh>
+
 #include <cfloat>
 #include <climits>
 #include <cmath>
@@ -81,6 +83,20 @@ __device__ __forceinline__ int ld_stream(const int *p)
 }
 
 __device__ __forceinline__ float ld_stream(const float *p) { return __int_as_float(ld_stream(reinterpret_cast<const int *>(p))); }
+
+// one light-row edge {target, weight bits}: a single 8-byte load
+__device__ __forceinline__ int2 ld_stream(const int2 *p)
+{
+#if TRAV_L2HINT
+    int2 v;
+    asm("ld.global.nc.L2::cache_hint.v2.s32 {%0, %1}, [%2], %3;"
+        : "=r"(v.x), "=r"(v.y)
+        : "l"(p), "l"(l2_policy_evict_first()));
+    return v;
+#else
+    return __ldg(p);
+#endif
+}
 
 // gather of a mutable word at L2 (bypassing L1), evict-last in L2
 __device__ __forceinline__ unsigned long long ld_gather(const unsigned long long *p)
@@ -492,6 +508,16 @@ __device__ void write_back(const TravArgs &a)
 // Flushes run once per 64-128 staged entries.  Out of line they shrink the
 // relaxation loop but force the pusher state into local memory, which costs
 // more (a 1024x1024 grid SSSP took 90 instead of 52 ms).
+// SSSP candidates are screened by the 16-bit distance filter (1) or by the
+// gathered 8-byte distance words (0); both give the same results.
+#ifndef TRAV_QFILTER
+#define TRAV_QFILTER 1
+#endif
+// SSSP light rounds read packed light rows (1) or the light prefixes of the
+// full rows (0); both give the same results.
+#ifndef TRAV_LIGHT_ROWS
+#define TRAV_LIGHT_ROWS 1
+#endif
 #ifndef TRAV_FLUSH_ATTR
 #define TRAV_FLUSH_ATTR __forceinline__
 #endif
@@ -566,6 +592,9 @@ struct Pusher {
 __device__ __forceinline__ int2 row_part(const TravArgs &a, int v, int part)
 {
     if (part == kPartIn) return make_int2(__ldg(&a.in_off[v]), __ldg(&a.in_off[v + 1]));
+    // light parts live in the light rows when the query has them (edge indices
+    // then count into a.ledge, not into out_adj / out_w)
+    if (part == kPartLight && a.loff) return make_int2(__ldg(&a.loff[v]), __ldg(&a.loff[v + 1]));
     int rb = __ldg(&a.out_off[v]), re = __ldg(&a.out_off[v + 1]);
     if (part == kPartLight) re = rb + __ldg(&a.nlight[v]);
     else if (part == kPartHeavy) rb += __ldg(&a.nlight[v]);
@@ -736,7 +765,7 @@ __device__ void expand_frontier(const TravArgs &a, const int32_t *q, unsigned nq
                 us[j] = u;
                 ds[j] = du;
             }
-            vis.visit_batch(us, ds, e, ok, p);
+            vis.template visit_batch<kPart>(us, ds, e, ok, p);
         }
     }
     WarpStage *s = p.s;
@@ -784,7 +813,7 @@ __device__ void expand_frontier(const TravArgs &a, const int32_t *q, unsigned nq
                 us[j] = s->tu[lo];
                 ds[j] = s->tdu[lo];
             }
-            vis.visit_batch(us, ds, e, ok, p);
+            vis.template visit_batch<kPart>(us, ds, e, ok, p);
         }
         __syncwarp();
     }
@@ -826,6 +855,7 @@ struct BfsPush {
         for (int j = 0; j < kBatch; j++) v[j] = ok[j] ? ld_stream(&a->out_adj[e[j]]) : 0;
     }
 
+    template <int kPart>
     __device__ __forceinline__ void visit_batch(const int (&)[kBatch], const float (&du)[kBatch],
                                                 const int (&e)[kBatch], const bool (&ok)[kBatch], Pusher &p) const
     {
@@ -914,9 +944,20 @@ struct SsspVisit {
 
     __device__ __forceinline__ float begin(int u) const { return dist_of(__ldcg(&a->dist[u])); }
 
+    template <int kPart>
     __device__ __forceinline__ void load_at(const int (&e)[kBatch], const bool (&ok)[kBatch], int (&v)[kBatch],
                                             float (&w)[kBatch]) const
     {
+        if (kPart == kPartLight && a->ledge) {
+            // light rows: target and weight of an edge side by side
+#pragma unroll
+            for (int j = 0; j < kBatch; j++) {
+                const int2 x = ok[j] ? ld_stream(&a->ledge[e[j]]) : make_int2(0, 0);
+                v[j] = x.x;
+                w[j] = __int_as_float(x.y);
+            }
+            return;
+        }
 #pragma unroll
         for (int j = 0; j < kBatch; j++) {
             v[j] = ok[j] ? ld_stream(&a->out_adj[e[j]]) : 0;
@@ -924,6 +965,7 @@ struct SsspVisit {
         }
     }
 
+    template <int kPart>
     __device__ __forceinline__ void visit_batch(const int (&us)[kBatch], const float (&du)[kBatch],
                                                 const int (&e)[kBatch], const bool (&ok)[kBatch], Pusher &p) const
     {
@@ -954,7 +996,7 @@ struct SsspVisit {
             }
             while (p.ndef >= 32) drain(p, 32);
         } else {
-            load_at(e, ok, v, w);
+            load_at<kPart>(e, ok, v, w);
             visit_loaded(du, v, w, ok, p);
         }
     }
@@ -976,15 +1018,25 @@ struct SsspVisit {
                                                  const float (&w)[kBatch], const bool (&ok)[kBatch], Pusher &p) const
     {
         float nd[kBatch];
+#if TRAV_QFILTER
         unsigned qv[kBatch];
 #pragma unroll
         for (int j = 0; j < kBatch; j++) qv[j] = ok[j] ? ld_gather_u16(&a->qd[v[j]]) : 0u;
+#else
+        unsigned long long qv[kBatch];  // the 8-byte distance words themselves
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) qv[j] = ok[j] ? ld_gather(&a->dist[v[j]]) : 0ull;
+#endif
 #pragma unroll
         for (int j = 0; j < kBatch; j++) nd[j] = ok[j] ? __fadd_rn(du[j], w[j]) : 0.0f;  // one rounded add, as sssp.hpp:56
         DeferStage *d = p.d;
 #pragma unroll
         for (int j = 0; j < kBatch; j++) {
+#if TRAV_QFILTER
             const bool cand = ok[j] && (unsigned)qd_of(nd[j]) <= qv[j];
+#else
+            const bool cand = ok[j] && nd[j] < dist_of(qv[j]);
+#endif
             const unsigned m = __ballot_sync(kFull, cand);
             if (cand) {
                 const unsigned i = p.ndef + __popc(m & lanemask_lt());
@@ -1627,6 +1679,8 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) batch_persistent
         a.chunks0 = w.chunks0;
         a.chunks1 = w.chunks1;
         a.nlight = q.nlight;
+        a.loff = q.loff;
+        a.ledge = q.ledge;
         a.source = q.source;
         a.out = q.out;
         a.mlp = q.mlp;
@@ -1838,6 +1892,19 @@ int persistent_grid_size(int kind)
     return g_grid[kind];
 }
 
+// Light rows: packed light prefixes {target, weight bits}, one warp per row.
+__global__ void light_fill_kernel(const int32_t *__restrict__ out_off, const int32_t *__restrict__ out_adj,
+                                  const float *__restrict__ out_w, const int32_t *__restrict__ nlight,
+                                  const int32_t *__restrict__ loff, int32_t V, int2 *__restrict__ ledge)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int v = warp; v < V; v += nwarps) {
+        const int rb = out_off[v], nl = nlight[v], lb = loff[v];
+        for (int k = (int)lane_id(); k < nl; k += 32)
+            ledge[lb + k] = make_int2(out_adj[rb + k], __float_as_int(out_w[rb + k]));
+    }
+}
+
 int count_light(const DevGraph &g, float delta, int32_t *nlight, cudaStream_t st)
 {
     int dev = 0, sms = 148;
@@ -1845,6 +1912,56 @@ int count_light(const DevGraph &g, float delta, int32_t *nlight, cudaStream_t st
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (g.V > 0) light_count_kernel<<<sms * 8, 256, 0, st>>>(g.out_off, g.out_w, g.V, delta, nlight);
     TRY_CUDA(cudaGetLastError());
+    return TRAV_OK;
+}
+
+void light_rows_free(LightRows *lr)
+{
+    cudaFree(lr->nlight);
+    cudaFree(lr->loff);
+    cudaFree(lr->ledge);
+    *lr = LightRows{};
+}
+
+// The light prefix of every row for delta (rows are sorted by weight), and with
+// TRAV_LIGHT_ROWS the prefixes packed into rows of their own: the light rounds
+// then read 8 contiguous bytes per edge, and a row's bounds from one array,
+// instead of two arrays and a prefix length.  Built once per (graph, delta).
+int light_rows_build(const DevGraph &g, float delta, LightRows *lr, cudaStream_t st)
+{
+    if (lr->delta == delta && lr->nlight) return TRAV_OK;
+    light_rows_free(lr);
+    const int32_t V = g.V > 0 ? g.V : 1;
+    TRY_CUDA(dev_malloc(&lr->nlight, sizeof(int32_t) * (size_t)V));
+    TRY(count_light(g, delta, lr->nlight, st));
+#if TRAV_LIGHT_ROWS
+    TRY_CUDA(dev_malloc(&lr->loff, sizeof(int32_t) * ((size_t)V + 1)));
+    // loff[0..V) = exclusive scan of nlight; loff[V] = the last offset plus the last length
+    size_t tmp_bytes = 0;
+    TRY_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, lr->nlight, lr->loff, V, st));
+    void *tmp = nullptr;
+    TRY_CUDA(dev_malloc(&tmp, tmp_bytes));
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, lr->nlight, lr->loff, g.V, st);
+    int32_t last[2] = {0, 0};
+    if (e == cudaSuccess && g.V > 0) e = cudaMemcpyAsync(&last[0], lr->loff + g.V - 1, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && g.V > 0) e = cudaMemcpyAsync(&last[1], lr->nlight + g.V - 1, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_fail(e, "light row offsets");
+    const int32_t total = last[0] + last[1];
+    TRY_CUDA(cudaMemcpyAsync(lr->loff + g.V, &total, sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    lr->edges = total;
+    TRY_CUDA(dev_malloc(&lr->ledge, sizeof(int2) * (size_t)(total > 0 ? total : 1)));
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g.V > 0)
+        light_fill_kernel<<<sms * 8, 256, 0, st>>>(g.out_off, g.out_adj, g.out_w, lr->nlight, lr->loff, g.V,
+                                                    lr->ledge);
+    TRY_CUDA(cudaGetLastError());
+    TRY_CUDA(cudaStreamSynchronize(st));  // the host value `total` is read by the copy above
+#endif
+    lr->delta = delta;
     return TRAV_OK;
 }
 
@@ -1893,7 +2010,6 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
         TRY_CUDA(dev_malloc(&ws->queue[i], sizeof(int32_t) * V));
         TRY_CUDA(dev_malloc(&ws->far[i], sizeof(int32_t) * V));
     }
-    TRY_CUDA(dev_malloc(&ws->nlight, sizeof(int32_t) * V));
     for (int i = 0; i < 2; i++) {
         TRY_CUDA(dev_malloc(&ws->hq[i], sizeof(int32_t) * V));
         TRY_CUDA(dev_malloc(&ws->hchunks[i], sizeof(int2) * ws->chunk_cap));
@@ -1902,7 +2018,6 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
     TRY_CUDA(dev_malloc(&ws->chunks[1], sizeof(int2) * ws->chunk_cap));
     TRY_CUDA(dev_malloc(&ws->ctl, sizeof(Ctl) * (size_t)nqueries));
     ws->ctl_cap = nqueries;
-    ws->nlight_delta = -1.0f;
     return TRAV_OK;
 }
 
@@ -1918,7 +2033,7 @@ void workspace_free(Workspace *ws)
         cudaFree(ws->queue[i]);
         cudaFree(ws->far[i]);
     }
-    cudaFree(ws->nlight);
+    light_rows_free(&ws->light);
     for (int i = 0; i < 2; i++) {
         cudaFree(ws->hq[i]);
         cudaFree(ws->hchunks[i]);
@@ -2014,11 +2129,10 @@ int launch_sssp(const DevGraph &g, Workspace *ws, int q, int32_t source_new, flo
         a.init_bits = reinterpret_cast<const unsigned *>(ws->queue[1]);
     }
     if (std::isfinite(a.delta)) {
-        if (ws->nlight_delta != a.delta) {  // rows are sorted by weight: count each light prefix once per delta
-            TRY(count_light(g, a.delta, ws->nlight, st));
-            ws->nlight_delta = a.delta;
-        }
-        a.nlight = ws->nlight;
+        TRY(light_rows_build(g, a.delta, &ws->light, st));  // once per delta
+        a.nlight = ws->light.nlight;
+        a.loff = ws->light.loff;
+        a.ledge = ws->light.ledge;
     }
     a.out = out;
     a.out_kind = out_kind;
