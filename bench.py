@@ -102,13 +102,6 @@ def pick_sources(deg, n, seed):
     return np.sort(rng.choice(cand, size=min(n, len(cand)), replace=False)).astype(np.int32)
 
 
-def e2e_cuts(n: int):
-    """Source boundaries of the e2e parts: 24/64, 20/64, 14/64 and 6/64 of n sources (fewer parts when n is
-    small), so that each part's result copy ends inside the next part's launch."""
-    frac = [24, 44, 58, 64]
-    return sorted(set([0] + [round(n * f / 64) for f in frac])) if n else [0]
-
-
 def rank_sources(deg, n, seed, rank):
     """Replica r of a weak-scaling run traverses its own seeded source set."""
     return pick_sources(deg, n, seed + rank)
@@ -468,26 +461,20 @@ def run_ours(a):
     assert np.array_equal(runs[primary]["lv"], lv_dev.cpu().numpy())
     assert np.array_equal(runs[primary]["di"].view(np.uint32), di_dev.cpu().numpy().view(np.uint32))
 
-    # e2e through the public API with pinned host buffers: per step, the query descriptors (source ids inside)
-    # go H2D in the call and every level / distance array comes back D2H.  The step runs as four launches over
-    # 24/64, 20/64, 14/64 and 6/64 of the sources; each part's results are copied on a second stream while the
-    # next part runs.  The parts shrink so that each copy still ends within the next part's launch (the copy of
-    # a part takes about 0.4 of its compute time) and only the small last part's copy is left after the last
-    # launch.  Timed on the host clock.
+    # e2e through the library's host-output batch call (trav_batch_run_host) with pinned host buffers: per step,
+    # the query descriptors (source ids inside) go H2D in the call and every level / distance array comes back
+    # D2H into the caller's host memory.  The library runs the 128 queries (each source's SSSP and BFS side by
+    # side) as four shrinking launches and copies each one's results while the next one runs.  Timed on the host
+    # clock.
     lv_host = torch.empty((n, V), dtype=torch.int32).pin_memory()
     di_host = torch.empty((n, V), dtype=torch.float32).pin_memory()
-    cs = torch.cuda.Stream()
-    cut = e2e_cuts(n)
-    parts = len(cut) - 1
-    chunks = [queries[primary][cut[i]:cut[i + 1]] + queries[primary][n + cut[i]:n + cut[i + 1]] for i in range(parts)]
+    host_queries = []
+    for i, s in enumerate(sources):
+        host_queries.append((0, 1, int(s), a.delta, primary, di_host[i]))
+        host_queries.append((0, 0, int(s), 0.0, primary, lv_host[i]))
 
     def e2e_step():
-        for i, q in enumerate(chunks):
-            batch.run(q)
-            with torch.cuda.stream(cs):
-                lv_host[cut[i]:cut[i + 1]].copy_(lv_dev[cut[i]:cut[i + 1]], non_blocking=True)
-                di_host[cut[i]:cut[i + 1]].copy_(di_dev[cut[i]:cut[i + 1]], non_blocking=True)
-        cs.synchronize()
+        batch.run_host(host_queries, parts=4)
 
     for _ in range(max(1, min(a.warmup, 2))):
         e2e_step()
@@ -540,7 +527,8 @@ def run_ours(a):
                          "queries_per_launch": len(queries[primary])},
             "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": 2 * 4 * n * V,
-                    "timing": "host clock around the batched C-ABI calls and the overlapped result copies"},
+                    "timing": "host clock around trav_batch_run_host (host output arrays; four launches, each "
+                              "one's results copied back while the next runs)"},
             "gpu_launches": a.steps,
             "ingest_s": ingest_s,
             "clocks": clk,

@@ -408,6 +408,20 @@ void trav_batch_free(trav_batch *b);
  * hold one per team, fewer teams of the same size run. */
 int trav_batch_run(trav_batch *b, const trav_query *queries, int32_t n, float *device_ms);
 
+/* The same queries with HOST output arrays (`out` = V results in host
+ * memory; pinned memory lets the copies overlap the work).  The queries run
+ * as `parts` launches over consecutive slices of the array, slices shrinking
+ * in the ratio 2 (parts - p) + 1; each slice's results are staged in device
+ * memory and copied to the host on a second stream while the next slice
+ * runs, so only the small last slice's copy follows the last launch.  Put
+ * mixed kinds side by side in the array (e.g. the BFS and SSSP queries of one
+ * source next to each other) so the slices balance.  *device_ms (may be
+ * NULL) receives the summed device time of the launches.  Returns after the
+ * last copy has finished.  The reference's counterpart is the per-call
+ * upload / kernel / copy-back of gpu_bellman_ford (algorithm/sssp/
+ * sssp.hpp:219-277). */
+int trav_batch_run_host(trav_batch *b, const trav_query *queries, int32_t n, int32_t parts, float *device_ms);
+
 /* Time candidate shapes on these queries (each run `reps` times, best kept)
  * and keep the fastest for later runs; *best (may be NULL) receives it. */
 int trav_batch_autotune(trav_batch *b, const trav_query *queries, int32_t n, int32_t reps,

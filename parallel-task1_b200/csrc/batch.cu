@@ -48,6 +48,11 @@ struct trav_batch {
     int q_cap = 0;
     unsigned *d_next = nullptr;
     std::map<std::pair<int, float>, LightRows> light;  // light rows per (graph, delta)
+    // host-output runs: device staging of the results and the copy stream
+    unsigned char *staging = nullptr;
+    size_t staging_bytes = 0;
+    cudaStream_t cst = nullptr;
+    cudaEvent_t part_done = nullptr;
     trav_batch_shape shape{16, kSmallDeg, kItem};
 };
 
@@ -327,6 +332,10 @@ void trav_batch_free(trav_batch *b)
     cudaFree(b->d_q);
     cudaFree(b->d_next);
     for (auto &kv : b->light) light_rows_free(&kv.second);
+    if (b->cst) cudaStreamSynchronize(b->cst);
+    cudaFree(b->staging);
+    if (b->part_done) cudaEventDestroy(b->part_done);
+    if (b->cst) cudaStreamDestroy(b->cst);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->st) cudaStreamDestroy(b->st);
@@ -345,6 +354,65 @@ int trav_batch_run(trav_batch *b, const trav_query *queries, int32_t n, float *d
         return TRAV_OK;
     }
     return run_launch(b, n, b->shape, device_ms);
+}
+
+int trav_batch_run_host(trav_batch *b, const trav_query *queries, int32_t n, int32_t parts, float *device_ms)
+{
+    if (!b) return bad("batch handle is NULL");
+    if (parts < 1) return bad("parts must be >= 1");
+    TRY_CUDA(cudaSetDevice(b->device));
+    for (trav_graph *g : b->graphs) TRY_CUDA(cudaStreamSynchronize(g->st));
+    TRY(check_queries_host(b, queries, n));
+    for (int32_t i = 0; i < n; i++)
+        if (is_device_ptr(queries[i].out)) return bad("trav_batch_run_host takes host output arrays (use trav_batch_run)");
+    if (device_ms) *device_ms = 0.0f;
+    if (n == 0) return TRAV_OK;
+    // every query's results get a slot in one device staging area
+    std::vector<size_t> at((size_t)n + 1, 0);
+    for (int32_t i = 0; i < n; i++)
+        at[(size_t)i + 1] = at[(size_t)i] + 4 * (size_t)b->graphs[(size_t)queries[i].graph]->g.V;
+    if (at[(size_t)n] > b->staging_bytes) {
+        if (b->cst) TRY_CUDA(cudaStreamSynchronize(b->cst));
+        cudaFree(b->staging);
+        b->staging = nullptr;
+        b->staging_bytes = 0;
+        TRY_CUDA(dev_malloc(&b->staging, at[(size_t)n]));
+        b->staging_bytes = at[(size_t)n];
+    }
+    if (!b->cst) TRY_CUDA(cudaStreamCreateWithFlags(&b->cst, cudaStreamNonBlocking));
+    if (!b->part_done) TRY_CUDA(cudaEventCreateWithFlags(&b->part_done, cudaEventDisableTiming));
+    std::vector<trav_query> dq(queries, queries + n);
+    for (int32_t i = 0; i < n; i++) dq[(size_t)i].out = b->staging + at[(size_t)i];
+    // Part p holds a share of the queries proportional to 2 (parts - p) + 1: the
+    // parts shrink, so each part's copy (about 0.4 of its compute at RMAT s23)
+    // ends inside the next part's launch and only a small last copy is left.
+    std::vector<int32_t> cut((size_t)parts + 1, 0);
+    double wsum = 0.0;
+    for (int p = 0; p < parts; p++) wsum += 2.0 * (parts - p) + 1.0;
+    double acc = 0.0;
+    for (int p = 0; p < parts; p++) {
+        acc += 2.0 * (parts - p) + 1.0;
+        cut[(size_t)p + 1] = (int32_t)std::lround(n * acc / wsum);
+    }
+    cut[(size_t)parts] = n;
+    float total = 0.0f;
+    for (int p = 0; p < parts; p++) {
+        const int32_t q0 = cut[(size_t)p], q1 = cut[(size_t)p + 1];
+        if (q1 <= q0) continue;
+        TRY(upload_queries(b, dq.data() + q0, q1 - q0));
+        float ms = 0.0f;
+        TRY(run_launch(b, q1 - q0, b->shape, &ms));
+        total += ms;
+        // the results of this part go to the host while the next part runs
+        TRY_CUDA(cudaEventRecord(b->part_done, b->st));
+        TRY_CUDA(cudaStreamWaitEvent(b->cst, b->part_done, 0));
+        for (int32_t i = q0; i < q1; i++)
+            TRY_CUDA(cudaMemcpyAsync(queries[i].out, b->staging + at[(size_t)i], at[(size_t)i + 1] - at[(size_t)i],
+                                     cudaMemcpyDeviceToHost, b->cst));
+    }
+    TRY_CUDA(cudaStreamSynchronize(b->cst));
+    if (device_ms) *device_ms = total;
+    return TRAV_OK;
 }
 
 int trav_batch_autotune(trav_batch *b, const trav_query *queries, int32_t n, int32_t reps, trav_batch_shape *best)

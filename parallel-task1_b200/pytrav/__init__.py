@@ -53,7 +53,7 @@ EXPORTS = [
     "trav_batch_autotune", "trav_batch_set_shape", "trav_batch_get_shape", "trav_graph_set_capture",
     "trav_el_optimize", "trav_el_gpu_transactions", "trav_adj_file_read", "trav_adj_file_write",
     "trav_pairs_file_read", "trav_set_limits", "trav_inject_alloc_failure", "trav_reach_el_masked",
-    "trav_mlp_set_margin",
+    "trav_mlp_set_margin", "trav_batch_run_host",
 ]
 
 
@@ -130,6 +130,7 @@ def lib():
         L.trav_batch_free.argtypes = [vp]
         L.trav_batch_free.restype = None
         L.trav_batch_run.argtypes = [vp, C.POINTER(Query), i32, C.POINTER(f32)]
+        L.trav_batch_run_host.argtypes = [vp, C.POINTER(Query), i32, i32, C.POINTER(f32)]
         L.trav_batch_autotune.argtypes = [vp, C.POINTER(Query), i32, i32, C.POINTER(BatchShape)]
         L.trav_batch_set_shape.argtypes = [vp, C.POINTER(BatchShape)]
         L.trav_batch_get_shape.argtypes = [vp, C.POINTER(BatchShape)]
@@ -529,11 +530,11 @@ class Batch:
             pass
 
     @staticmethod
-    def _queries(queries):
+    def _queries(queries, host=False):
         qs = list(queries)
         arr = (Query * max(1, len(qs)))()
         for i, (gi, kind, src, delta, sched, out) in enumerate(qs):
-            assert _is_cuda(out), "batch results must be CUDA tensors"
+            assert _is_cuda(out) != host, "batch results must be " + ("host arrays" if host else "CUDA tensors")
             arr[i] = Query(gi, kind, int(src), float(delta), sched, _ptr(out))
         return arr, len(qs)
 
@@ -542,6 +543,14 @@ class Batch:
         arr, n = self._queries(queries)
         ms = C.c_float(0.0)
         _check(lib().trav_batch_run(self._h, arr, n, C.byref(ms)))
+        return ms.value
+
+    def run_host(self, queries, parts: int = 4) -> float:
+        """Run queries whose `out` is host memory (pinned tensors or numpy arrays) as `parts` shrinking launches,
+        each part's results copied back while the next part runs; returns the summed device time in ms."""
+        arr, n = self._queries(queries, host=True)
+        ms = C.c_float(0.0)
+        _check(lib().trav_batch_run_host(self._h, arr, n, parts, C.byref(ms)))
         return ms.value
 
     def autotune(self, queries, reps: int = 2):

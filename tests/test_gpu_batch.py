@@ -137,3 +137,42 @@ def test_batch_errors(batch_case):
         b.shape = (4, 32, 32)
     assert b.run([]) == 0.0
     b.close()
+
+
+@pytest.mark.parametrize("parts", [1, 3, 4])
+def test_host_output_batch_equals_device_output_batch(parts):
+    """trav_batch_run_host (host output arrays, shrinking launches with overlapped copies) gives the results
+    of trav_batch_run, and the oracle's."""
+    import torch
+
+    s, d, w = O.rmat(12, 16, seed=31)
+    V = 1 << 12
+    g = T.Graph.from_edges(V, s, d, w)
+    deg = np.bincount(s, minlength=V)
+    srcs = [int(x) for x in np.flatnonzero(deg > 0)[[0, 5, 77, 301, 902]]]
+    dev_q, host_q, host_out = [], [], []
+    for src in srcs:
+        for kind in (1, 0):
+            dt = torch.float32 if kind == 1 else torch.int32
+            dev_q.append((0, kind, src, 0.1, T.SCHEDULE_PLAIN, torch.empty(V, dtype=dt, device="cuda")))
+            h = torch.full((V,), 3, dtype=dt).pin_memory() if parts != 3 else np.full(V, 3, np.float32 if kind else np.int32)
+            host_out.append(h)
+            host_q.append((0, kind, src, 0.1, T.SCHEDULE_PLAIN, h))
+    b = T.Batch([g])
+    b.run(dev_q)
+    ms = b.run_host(host_q, parts=parts)
+    assert ms > 0
+    for (gi, kind, src, _, _, dv), h in zip(dev_q, host_out):
+        got = h.numpy() if hasattr(h, "numpy") else h
+        assert np.array_equal(got.view(np.uint32), dv.cpu().numpy().view(np.uint32)), (kind, src)
+        if kind == 1:
+            assert np.array_equal(got.view(np.uint32), O.bellman_ford(V, s, d, w, src).view(np.uint32))
+        else:
+            assert np.array_equal(got, O.bfs_levels(V, s, d, src))
+    # a device output array is refused by the library itself
+    import ctypes as C
+    arr = (T.Query * 1)(T.Query(0, 1, srcs[0], 0.1, T.SCHEDULE_PLAIN, dev_q[0][5].data_ptr()))
+    ms_out = C.c_float()
+    assert T.lib().trav_batch_run_host(b._h, arr, 1, 2, C.byref(ms_out)) == T.TRAV_ERR_BAD_ARG
+    b.close()
+    g.free()
