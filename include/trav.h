@@ -422,8 +422,21 @@ int trav_batch_run(trav_batch *b, const trav_query *queries, int32_t n, float *d
  * sssp.hpp:219-277). */
 int trav_batch_run_host(trav_batch *b, const trav_query *queries, int32_t n, int32_t parts, float *device_ms);
 
+/* Process-wide table of the launch shapes the autotuner found, keyed by the
+ * kind of batch: the device's co-resident CTAs, log2 of the largest queried
+ * graph's V and E, log2 of the number of graphs and queries, and the shares
+ * of SSSP and learned-schedule queries in eighths.  save writes it as text
+ * lines "key team_ctas small_deg item"; load merges a saved table into the
+ * current one (*entries, may be NULL, receives its size).  Malformed files
+ * are rejected with TRAV_ERR_IO.  New; the reference has no autotuner. */
+int trav_tune_table_save(const char *path);
+int trav_tune_table_load(const char *path, int32_t *entries);
+
 /* Time candidate shapes on these queries (each run `reps` times, best kept)
- * and keep the fastest for later runs; *best (may be NULL) receives it. */
+ * and keep the fastest for later runs; *best (may be NULL) receives it.  The
+ * result is also recorded in the tuning table.  reps == 0 takes the table's
+ * shape for this kind of batch without timing anything, and tunes once
+ * (reps 1) when the table has none. */
 int trav_batch_autotune(trav_batch *b, const trav_query *queries, int32_t n, int32_t reps,
                         trav_batch_shape *best);
 

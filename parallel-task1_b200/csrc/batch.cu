@@ -7,7 +7,9 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdio>
 #include <map>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <utility>
@@ -282,6 +284,42 @@ int upload_queries(trav_batch *b, const trav_query *qs, int32_t n)
     return TRAV_OK;
 }
 
+// Launch shapes the autotuner found, process-wide, by kind of batch
+// (trav_tune_table_save / _load persist them).
+std::map<std::string, trav_batch_shape> g_tune_table;
+std::mutex g_tune_mu;
+
+int ceil_log2(int64_t x)
+{
+    int k = 0;
+    while (k < 62 && ((int64_t)1 << k) < x) k++;
+    return k;
+}
+
+// What the best launch shape depends on: the device (its co-resident CTAs),
+// the size of the largest graph queried, the number of graphs and queries,
+// and the shares of SSSP and learned-schedule queries (in eighths).
+std::string tune_key(const trav_batch *b, const trav_query *qs, int32_t n, int most)
+{
+    int64_t vmax = 1, emax = 1;
+    int sssp = 0, learned = 0;
+    std::vector<char> used(b->graphs.size(), 0);
+    for (int32_t i = 0; i < n; i++) {
+        const trav_graph *g = b->graphs[(size_t)qs[i].graph];
+        used[(size_t)qs[i].graph] = 1;
+        vmax = std::max<int64_t>(vmax, g->g.V);
+        emax = std::max<int64_t>(emax, g->g.E);
+        sssp += qs[i].kind == 1;
+        learned += qs[i].schedule == TRAV_SCHEDULE_LEARNED;
+    }
+    const int graphs = (int)std::count(used.begin(), used.end(), 1);
+    const int nn = std::max(n, 1);
+    return "ctas" + std::to_string(most) + "_v" + std::to_string(ceil_log2(vmax)) + "_e" +
+           std::to_string(ceil_log2(emax)) + "_g" + std::to_string(ceil_log2(graphs)) + "_q" +
+           std::to_string(ceil_log2(nn)) + "_s" + std::to_string(8 * sssp / nn) + "_l" +
+           std::to_string(8 * learned / nn);
+}
+
 }  // namespace
 
 extern "C" {
@@ -418,12 +456,25 @@ int trav_batch_run_host(trav_batch *b, const trav_query *queries, int32_t n, int
 int trav_batch_autotune(trav_batch *b, const trav_query *queries, int32_t n, int32_t reps, trav_batch_shape *best)
 {
     if (!b) return bad("batch handle is NULL");
-    if (reps < 1) return bad("reps must be >= 1");
+    if (reps < 0) return bad("reps must be >= 0");
     TRY_CUDA(cudaSetDevice(b->device));
     for (trav_graph *g : b->graphs) TRY_CUDA(cudaStreamSynchronize(g->st));
-    TRY(upload_queries(b, queries, n));
+    TRY(check_queries_host(b, queries, n));
     const int most = persistent_grid_size(2);
     if (most <= 0) return TRAV_ERR_CUDA;
+    const std::string key = tune_key(b, queries, n, most);
+    if (reps == 0 && n > 0) {
+        // a shape tuned earlier for this kind of batch on this kind of device
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune_table.find(key);
+        if (it != g_tune_table.end() && shape_ok(it->second, most) == TRAV_OK) {
+            b->shape = it->second;
+            if (best) *best = b->shape;
+            return TRAV_OK;
+        }
+    }
+    if (reps == 0) reps = 1;
+    TRY(upload_queries(b, queries, n));
     if (n > 0) {
         auto time_of = [&](const trav_batch_shape &s, float *t) {
             float m = INFINITY;
@@ -473,8 +524,61 @@ int trav_batch_autotune(trav_batch *b, const trav_query *queries, int32_t n, int
             }
         }
         b->shape = cur;
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune_table[key] = cur;
     }
     if (best) *best = b->shape;
+    return TRAV_OK;
+}
+
+int trav_tune_table_save(const char *path)
+{
+    if (!path) return bad("path must not be NULL");
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    FILE *f = fopen(path, "w");
+    if (!f) {
+        set_error(std::string("cannot create ") + path);
+        return TRAV_ERR_IO;
+    }
+    fprintf(f, "# trav-b200 batch launch shapes: key team_ctas small_deg item\n");
+    for (const auto &kv : g_tune_table)
+        fprintf(f, "%s %d %d %d\n", kv.first.c_str(), kv.second.team_ctas, kv.second.small_deg, kv.second.item);
+    const bool ok = fclose(f) == 0;
+    if (!ok) {
+        set_error(std::string("write failed: ") + path);
+        return TRAV_ERR_IO;
+    }
+    return TRAV_OK;
+}
+
+int trav_tune_table_load(const char *path, int32_t *entries)
+{
+    if (!path) return bad("path must not be NULL");
+    FILE *f = fopen(path, "r");
+    if (!f) {
+        set_error(std::string("cannot open ") + path);
+        return TRAV_ERR_IO;
+    }
+    std::map<std::string, trav_batch_shape> got;
+    char line[512];
+    int lineno = 0;
+    while (fgets(line, sizeof line, f)) {
+        lineno++;
+        if (line[0] == '#' || line[0] == '\n') continue;
+        char key[256];
+        trav_batch_shape s{};
+        if (sscanf(line, "%255s %d %d %d", key, &s.team_ctas, &s.small_deg, &s.item) != 4 || s.team_ctas < 1 ||
+            s.small_deg < 0 || s.small_deg > kMaxSmallDeg || s.item < kMinItem || s.item > kMaxItem) {
+            fclose(f);
+            set_error(std::string("malformed tuning table line ") + std::to_string(lineno) + " in " + path);
+            return TRAV_ERR_IO;
+        }
+        got[key] = s;
+    }
+    fclose(f);
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    for (const auto &kv : got) g_tune_table[kv.first] = kv.second;
+    if (entries) *entries = (int32_t)g_tune_table.size();
     return TRAV_OK;
 }
 

@@ -84,10 +84,16 @@ __device__ __forceinline__ int ld_stream(const int *p)
 
 __device__ __forceinline__ float ld_stream(const float *p) { return __int_as_float(ld_stream(reinterpret_cast<const int *>(p))); }
 
-// one light-row edge {target, weight bits}: a single 8-byte load
+// one light-row edge {target, weight bits}: a single 8-byte load.  The light
+// rows are re-read by every light round and by every concurrent query on the
+// graph; TRAV_LIGHT_KEEP leaves them at the normal L2 priority instead of
+// marking them evict-first like the other edge streams.
+#ifndef TRAV_LIGHT_KEEP
+#define TRAV_LIGHT_KEEP 0
+#endif
 __device__ __forceinline__ int2 ld_stream(const int2 *p)
 {
-#if TRAV_L2HINT
+#if TRAV_L2HINT && !TRAV_LIGHT_KEEP
     int2 v;
     asm("ld.global.nc.L2::cache_hint.v2.s32 {%0, %1}, [%2], %3;"
         : "=r"(v.x), "=r"(v.y)

@@ -53,7 +53,7 @@ EXPORTS = [
     "trav_batch_autotune", "trav_batch_set_shape", "trav_batch_get_shape", "trav_graph_set_capture",
     "trav_el_optimize", "trav_el_gpu_transactions", "trav_adj_file_read", "trav_adj_file_write",
     "trav_pairs_file_read", "trav_set_limits", "trav_inject_alloc_failure", "trav_reach_el_masked",
-    "trav_mlp_set_margin", "trav_batch_run_host",
+    "trav_mlp_set_margin", "trav_batch_run_host", "trav_tune_table_save", "trav_tune_table_load",
 ]
 
 
@@ -132,6 +132,8 @@ def lib():
         L.trav_batch_run.argtypes = [vp, C.POINTER(Query), i32, C.POINTER(f32)]
         L.trav_batch_run_host.argtypes = [vp, C.POINTER(Query), i32, i32, C.POINTER(f32)]
         L.trav_batch_autotune.argtypes = [vp, C.POINTER(Query), i32, i32, C.POINTER(BatchShape)]
+        L.trav_tune_table_save.argtypes = [C.c_char_p]
+        L.trav_tune_table_load.argtypes = [C.c_char_p, C.POINTER(i32)]
         L.trav_batch_set_shape.argtypes = [vp, C.POINTER(BatchShape)]
         L.trav_batch_get_shape.argtypes = [vp, C.POINTER(BatchShape)]
         L.trav_mlp_param_count.argtypes = [i32]
@@ -554,7 +556,8 @@ class Batch:
         return ms.value
 
     def autotune(self, queries, reps: int = 2):
-        """Time candidate launch shapes on these queries; keeps and returns the fastest (team_ctas, small_deg, item)."""
+        """Time candidate launch shapes on these queries; keeps and returns the fastest (team_ctas, small_deg, item).
+        reps=0 takes the tuning table's shape for this kind of batch when it has one."""
         arr, n = self._queries(queries)
         best = BatchShape()
         _check(lib().trav_batch_autotune(self._h, arr, n, reps, C.byref(best)))
@@ -586,4 +589,20 @@ def el_gpu_transactions(src, dst, vertices: int, elem_size: int = 4) -> int:
     n = C.c_int64(0)
     mem = MEM_DEVICE if _is_cuda(src) else MEM_HOST
     _check(lib().trav_el_gpu_transactions(_ptr(src), _ptr(dst), vertices, len(src), elem_size, mem, C.byref(n)))
+    return n.value
+
+
+# ------------------------------------------------------- launch-shape table
+TUNE_TABLE = os.path.join(PKG, "weights", "batch_shapes.txt")
+
+
+def tune_table_save(path: str = TUNE_TABLE):
+    """Write the process's table of autotuned batch launch shapes."""
+    _check(lib().trav_tune_table_save(path.encode()))
+
+
+def tune_table_load(path: str = TUNE_TABLE) -> int:
+    """Merge a saved table of batch launch shapes into the process's; returns the table's size."""
+    n = C.c_int32(0)
+    _check(lib().trav_tune_table_load(path.encode(), C.byref(n)))
     return n.value

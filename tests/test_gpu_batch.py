@@ -103,6 +103,11 @@ def test_batch_autotune_picks_a_valid_shape(batch_case):
     b.run(queries)
     _check(queries, want)
     b.close()
+    # the tuned shape went into the table: a new batch of the same kind takes it without timing
+    b2 = T.Batch(graphs)
+    b2.shape = (1, 8, 1024)
+    assert b2.autotune(queries, reps=0) == best
+    b2.close()
 
 
 def test_batch_equals_single_query_api(batch_case):

@@ -121,3 +121,22 @@ def test_noalloc_bfs_refuses_host_pointers_without_launching():
     with pytest.raises(T.TravError) as e:
         T.bfs_csr_noalloc(off, adj, 2, 1, 0, lv)
     assert e.value.code == T.TRAV_ERR_BAD_ARG and "device" in str(e.value)
+
+
+def test_tune_table_round_trip_and_rejects_malformed_files(tmp_path):
+    """The autotuner's persisted shape table is host-only: load merges, save writes the same lines back."""
+    good = tmp_path / "shapes.txt"
+    good.write_text("# comment\nctas592_v23_e28_g0_q7_s4_l8 74 64 256\nctas592_v18_e23_g6_q9_s4_l0 8 32 128\n")
+    assert T.tune_table_load(str(good)) >= 2
+    out = tmp_path / "again.txt"
+    T.tune_table_save(str(out))
+    lines = [line for line in out.read_text().splitlines() if not line.startswith("#")]
+    assert "ctas592_v23_e28_g0_q7_s4_l8 74 64 256" in lines and "ctas592_v18_e23_g6_q9_s4_l0 8 32 128" in lines
+    for bad in ("key 74 64\n", "key 0 32 128\n", "key 8 32 99999\n"):
+        p = tmp_path / "bad.txt"
+        p.write_text(bad)
+        with pytest.raises(T.TravError) as e:
+            T.tune_table_load(str(p))
+        assert e.value.code == T.TRAV_ERR_IO
+    with pytest.raises(T.TravError):
+        T.tune_table_load(str(tmp_path / "missing.txt"))
