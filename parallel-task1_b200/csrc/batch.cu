@@ -70,7 +70,7 @@ size_t round_up(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Byte layout of one team's scratch (every array 256-byte aligned).
 struct TeamLayout {
-    size_t value, qd, rcls, visited, front0, front1, q[6], chunks[4], total;
+    size_t value, rcls, visited, front0, front1, q[6], chunks[4], total;
 };
 
 TeamLayout team_layout(const trav_batch *b)
@@ -83,7 +83,6 @@ TeamLayout team_layout(const trav_batch *b)
         return at;
     };
     L.value = take(sizeof(unsigned long long) * (size_t)b->vmax);
-    L.qd = take(sizeof(unsigned short) * (size_t)b->vmax);
     L.rcls = take(sizeof(unsigned char) * (size_t)b->vmax);
     L.visited = take(sizeof(unsigned) * (size_t)b->wmax);
     L.front0 = take(sizeof(unsigned) * (size_t)b->wmax);
@@ -115,7 +114,6 @@ int ensure_teams(trav_batch *b, int teams)
         unsigned char *m = b->team_mem + L.total * (size_t)t;
         TeamWs &w = h[(size_t)t];
         w.value = reinterpret_cast<unsigned *>(m + L.value);
-        w.qd = reinterpret_cast<unsigned short *>(m + L.qd);
         w.rcls = m + L.rcls;
         w.visited = reinterpret_cast<unsigned *>(m + L.visited);
         w.front0 = reinterpret_cast<unsigned *>(m + L.front0);

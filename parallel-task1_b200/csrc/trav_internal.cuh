@@ -23,18 +23,14 @@ constexpr int kMaxDec = 1024;     // schedule decisions recorded per query
 constexpr int kDecFeat = 10;      // features per decision (the schedule MLP's input width)
 constexpr int kSlots = 4;         // ring of per-phase counter slots
 constexpr unsigned long long kDefaultTimeoutNs = 10ull * 1000000000ull;  // grid-barrier wait limit (10 s)
-// Row-class flags of a vertex for SSSP (one byte per vertex, written at a
-// query's initialisation): which parts of its out-row are non-empty and which
-// are longer than the warp-tile threshold.  They depend only on the graph and
-// delta.  An SSSP distance word is dist_bits << 32 | round << kClsBits; its
-// low kClsBits bits stay zero.
+// Row-class flags in the low bits of an SSSP distance word (dist_bits << 32 |
+// round << kClsBits | flags): which parts of the vertex's out-row are non-empty
+// and which are longer than the warp-tile threshold.  They depend only on the
+// graph and delta, so the 64-bit atomicMin that lowers a distance keeps them.
+// A copy in one byte per vertex (written at a query's initialisation) serves
+// the pull rounds, which gather no word of the vertex they improve.
 constexpr unsigned kClsLight = 1, kClsLightBig = 2, kClsHeavy = 4, kClsHeavyBig = 8;
 constexpr unsigned kClsBits = 4, kClsMask = (1u << kClsBits) - 1u;
-// Distance filter of SSSP: qd[v] >= (bits of v's distance) >> kQdShift at all
-// times (0xFFFF while v is unreached), a 16-bit upper bound on the distance's
-// quantised bits.  A candidate whose quantised bits exceed it cannot lower v.
-constexpr unsigned kQdShift = 15;
-constexpr unsigned short kQdUnreached = 0xFFFFu;
 constexpr int kMaxRounds = (1 << (32 - kClsBits)) - 1;  // round ids of one SSSP launch must fit the stamp
 
 // Device status codes written to Ctl::err.
@@ -122,10 +118,9 @@ struct Workspace {
     int32_t V = 0;
     int64_t chunk_cap = 0;
     // V 64-bit words: BFS levels (int32, the first V words) or SSSP distance
-    // words (float bits << 32 | round << kClsBits)
+    // words (float bits << 32 | round << kClsBits | row-class flags)
     unsigned int *value = nullptr;
-    unsigned short *qd = nullptr;      // V: SSSP distance filter (see kQdShift)
-    unsigned char *rcls = nullptr;     // V: SSSP row-class flags
+    unsigned char *rcls = nullptr;     // V: SSSP row-class flags (the pull rounds' copy)
     unsigned int *visited = nullptr;   // W words
     unsigned int *front[2] = {nullptr, nullptr};  // W words each
     int32_t *queue[2] = {nullptr, nullptr};       // V each
@@ -162,8 +157,7 @@ struct TravArgs {
     // workspace
     unsigned int *value;        // BFS levels
     unsigned long long *dist;   // SSSP distance words (same memory as value)
-    unsigned short *qd;         // SSSP distance filter (see kQdShift)
-    unsigned char *rcls;        // SSSP row-class flags of each vertex
+    unsigned char *rcls;        // SSSP row-class flags of each vertex (pull rounds)
     unsigned int *visited;
     unsigned int *front0, *front1;
     int32_t *q0, *q1;
@@ -233,7 +227,6 @@ struct BatchQuery {
 // Scratch of one team of a batch launch, sized for the batch's largest graph.
 struct TeamWs {
     unsigned int *value;  // 2 * Vmax words
-    unsigned short *qd;   // Vmax
     unsigned char *rcls;  // Vmax
     unsigned int *visited, *front0, *front1;
     int32_t *q0, *q1, *far0, *far1, *hq0, *hq1;

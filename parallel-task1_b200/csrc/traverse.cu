@@ -116,22 +116,6 @@ __device__ __forceinline__ unsigned long long ld_gather(const unsigned long long
 #endif
 }
 
-// gather of a mutable 16-bit filter entry at L2, evict-last: the filter array
-// (2 bytes per vertex) is meant to stay L2-resident while the 8-byte distance
-// words it screens are touched only by the atomics of candidates
-__device__ __forceinline__ unsigned ld_gather_u16(const unsigned short *p)
-{
-#if TRAV_L2HINT
-    unsigned short v;
-    asm volatile("ld.global.cg.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(l2_policy_evict_last()));
-    return v;
-#else
-    return __ldcg(p);
-#endif
-}
-
-__device__ __forceinline__ unsigned short qd_of(float d) { return (unsigned short)(__float_as_uint(d) >> kQdShift); }
-
 __device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned *p)
 {
     unsigned v;
@@ -514,11 +498,6 @@ __device__ void write_back(const TravArgs &a)
 // Flushes run once per 64-128 staged entries.  Out of line they shrink the
 // relaxation loop but force the pusher state into local memory, which costs
 // more (a 1024x1024 grid SSSP took 90 instead of 52 ms).
-// SSSP candidates are screened by the 16-bit distance filter (1) or by the
-// gathered 8-byte distance words (0); both give the same results.
-#ifndef TRAV_QFILTER
-#define TRAV_QFILTER 1
-#endif
 // SSSP light rounds read packed light rows (1) or the light prefixes of the
 // full rows (0); both give the same results.
 #ifndef TRAV_LIGHT_ROWS
@@ -558,9 +537,19 @@ struct WarpStage {
 // Deferred SSSP relaxations of one warp (see SsspPush): fewer than 32 kept
 // between batches, plus up to 32 per edge of a lane's batch.
 constexpr int kWDefer = 32 + 32 * kBatchSssp;
+// Where a drain takes a candidate's row-class flags from: the gathered
+// distance word, staged with the candidate (0), or the byte array, loaded in
+// parallel with the atomic (1).  Same results either way; the byte frees the
+// registers and shared memory of the staged flags.
+#ifndef TRAV_CLS_BYTE
+#define TRAV_CLS_BYTE 1
+#endif
 struct DeferStage {
     int v[kWDefer];
     float d[kWDefer];
+#if !TRAV_CLS_BYTE
+    unsigned cls[kWDefer];
+#endif
 };
 
 struct CtaCounters {
@@ -1007,47 +996,35 @@ struct SsspVisit {
         }
     }
 
-    // An edge is screened by the target's 16-bit distance filter, not by its
-    // 8-byte distance word: qd[v] is an upper bound on the quantised bits of
-    // v's distance, so a candidate whose quantised bits exceed it cannot lower
-    // v and is dropped.  The filter array (2 bytes per vertex) stays in L2,
-    // where the distance words of a batch's concurrent queries do not fit.
-    // Any other candidate is not relaxed at once: (v, candidate) goes to the
-    // warp's DeferStage, and the atomicMins run 32 at a time (drain).  A batch
-    // then waits on its edge loads and its filter gathers only; the wait for
-    // an atomic's return comes once per 32 candidates.  The candidates are
-    // relaxed within the same phase, and the push decision reads only the
-    // atomic's return value, so the order of the atomics changes nothing; a
-    // candidate the filter lets through that does not improve v is refused by
-    // its atomicMin.
+    // An edge whose candidate beats the gathered distance is not relaxed at
+    // once: (v, candidate, row class) goes to the warp's DeferStage, and the
+    // atomicMins run 32 at a time (drain).  A batch then waits on its edge
+    // loads and its gathers only; the wait for an atomic's return -- which
+    // every batch used to pay, since almost every batch of 32 * kBatch edges
+    // has an improving lane -- comes once per 32 candidates.  The candidates
+    // are relaxed within the same phase, and the push decision reads only the
+    // atomic's return value, so the order of the atomics changes nothing.
     __device__ __forceinline__ void visit_loaded(const float (&du)[kBatch], const int (&v)[kBatch],
                                                  const float (&w)[kBatch], const bool (&ok)[kBatch], Pusher &p) const
     {
         float nd[kBatch];
-#if TRAV_QFILTER
-        unsigned qv[kBatch];
-#pragma unroll
-        for (int j = 0; j < kBatch; j++) qv[j] = ok[j] ? ld_gather_u16(&a->qd[v[j]]) : 0u;
-#else
-        unsigned long long qv[kBatch];  // the 8-byte distance words themselves
-#pragma unroll
-        for (int j = 0; j < kBatch; j++) qv[j] = ok[j] ? ld_gather(&a->dist[v[j]]) : 0ull;
-#endif
+        unsigned long long cur[kBatch];
 #pragma unroll
         for (int j = 0; j < kBatch; j++) nd[j] = ok[j] ? __fadd_rn(du[j], w[j]) : 0.0f;  // one rounded add, as sssp.hpp:56
+#pragma unroll
+        for (int j = 0; j < kBatch; j++) cur[j] = ok[j] ? ld_gather(&a->dist[v[j]]) : 0ull;
         DeferStage *d = p.d;
 #pragma unroll
         for (int j = 0; j < kBatch; j++) {
-#if TRAV_QFILTER
-            const bool cand = ok[j] && (unsigned)qd_of(nd[j]) <= qv[j];
-#else
-            const bool cand = ok[j] && nd[j] < dist_of(qv[j]);
-#endif
+            const bool cand = ok[j] && nd[j] < dist_of(cur[j]);
             const unsigned m = __ballot_sync(kFull, cand);
             if (cand) {
                 const unsigned i = p.ndef + __popc(m & lanemask_lt());
                 d->v[i] = v[j];
                 d->d[i] = nd[j];
+#if !TRAV_CLS_BYTE
+                d->cls[i] = (unsigned)cur[j] & kClsMask;
+#endif
             }
             p.ndef += __popc(m);
         }
@@ -1070,25 +1047,28 @@ struct SsspVisit {
         const bool ok = lane < n;
         int v = 0;
         float nd = 0.0f;
+        unsigned cls = 0;
         if (ok) {
             v = d->v[base + lane];
             nd = d->d[base + lane];
+#if !TRAV_CLS_BYTE
+            if constexpr (!kPull) cls = d->cls[base + lane];
+#endif
         }
         __syncwarp();  // the entries are read before later batches overwrite them
+        if (kPull || TRAV_CLS_BYTE) {
+            // the flags' byte copy (a pull stages no gathered word of the vertex
+            // it improves): written at this query's initialisation, by other
+            // CTAs and per query in a team, so read at L2 rather than through
+            // the read-only path
+            if (ok) cls = __ldcg(&a->rcls[v]);
+        }
         p.ndef = base;
         bool light = false, heavy = false, far = false;
-        unsigned cls = 0;
         if (ok) {
-            // written at this query's initialisation (by other CTAs, and a team
-            // rewrites it per query): read at L2, not through the read-only
-            // path; independent of the atomic, so both round trips overlap
-            cls = __ldcg(&a->rcls[v]);
-            const unsigned long long old = atomicMin(&a->dist[v], pack_dist(nd, round << kClsBits));
+            const unsigned long long old = atomicMin(&a->dist[v], pack_dist(nd, round << kClsBits | cls));
             const float od = dist_of(old);
             if (nd < od) {
-                // nd is now an upper bound of v's distance; a racing store of a
-                // larger bound only lets more candidates through
-                a->qd[v] = qd_of(nd);
                 const unsigned orr = (unsigned)old >> kClsBits;
                 if (nd < thr) {
                     const bool seen_below = od < thr;
@@ -1381,9 +1361,9 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
     if (a.source >= 0) {
         const int s = a.source;
         for (int v = gtid; v < a.V; v += nth) {
-            a.rcls[v] = (unsigned char)row_class(a, v);
-            a.dist[v] = pack_dist(v == s ? 0.0f : FLT_MAX, 0u);
-            a.qd[v] = v == s ? (unsigned short)0 : kQdUnreached;
+            const unsigned cls = row_class(a, v);
+            a.rcls[v] = (unsigned char)cls;
+            a.dist[v] = pack_dist(v == s ? 0.0f : FLT_MAX, cls);
         }
         const int2 lp = row_part(a, s, lpart);
         seed_part(a, s, lp.x, lp.y, a.q0, a.chunks0, nq, nch);
@@ -1412,8 +1392,7 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
                 bits = __ldg(&a.init_bits[v]);
                 cls = row_class(a, v);
                 a.rcls[v] = (unsigned char)cls;
-                a.dist[v] = static_cast<unsigned long long>(bits) << 32;
-                a.qd[v] = bits < kFltMaxBits ? (unsigned short)(bits >> kQdShift) : kQdUnreached;
+                a.dist[v] = (static_cast<unsigned long long>(bits) << 32) | cls;
             }
             const bool act = bits < kFltMaxBits && (cls & kClsLight);
             push(p, 0, act, v, cls & kClsLightBig ? big_len : 1u);
@@ -1577,14 +1556,14 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
                 const bool valid = i < far_len;
                 const int v = valid ? fp[i] : 0;
                 const unsigned long long dv = valid ? __ldcg(&a.dist[v]) : 0ull;
-                const unsigned cls = valid ? __ldcg(&a.rcls[v]) : 0u;
+                const unsigned cls = (unsigned)dv & kClsMask;
                 const float d = dist_of(dv);
                 const bool in_bucket = valid && d >= told && d < thr;
                 // the pile holds each vertex once (see SsspPush), so every entry is pushed on
                 const bool light = in_bucket && (cls & kClsLight);
                 const bool heavy = in_bucket && (cls & kClsHeavy);
                 const bool keep = valid && d >= thr;
-                if (in_bucket || keep) atomicMax(&a.dist[v], pack_dist(d, round << kClsBits));
+                if (in_bucket || keep) atomicMax(&a.dist[v], pack_dist(d, round << kClsBits | cls));
                 push(p, 0, light, v, cls & kClsLightBig ? big_len : 1u);
                 push(p, 1, heavy, v, cls & kClsHeavyBig ? big_len : 1u);
                 push_far(p, keep, v, keep ? 0x7fffffff - __float_as_int(d) : 0);
@@ -1668,7 +1647,6 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) batch_persistent
         a.E = q.E;
         a.value = w.value;
         a.dist = reinterpret_cast<unsigned long long *>(w.value);
-        a.qd = w.qd;
         a.rcls = w.rcls;
         a.visited = w.visited;
         a.front0 = w.front0;
@@ -2006,7 +1984,6 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
     ws->V = g.V;
     ws->chunk_cap = V + g.E / kMinItem + 1;
     TRY_CUDA(dev_malloc(&ws->value, sizeof(unsigned long long) * V));
-    TRY_CUDA(dev_malloc(&ws->qd, sizeof(unsigned short) * V));
     TRY_CUDA(dev_malloc(&ws->rcls, sizeof(unsigned char) * V));
 
     TRY_CUDA(dev_malloc(&ws->visited, sizeof(unsigned) * W));
@@ -2030,7 +2007,6 @@ int workspace_ensure(Workspace *ws, const DevGraph &g, int nqueries, cudaStream_
 void workspace_free(Workspace *ws)
 {
     cudaFree(ws->value);
-    cudaFree(ws->qd);
     cudaFree(ws->rcls);
     cudaFree(ws->visited);
     cudaFree(ws->front[0]);
@@ -2067,7 +2043,6 @@ static TravArgs make_args(const DevGraph &g, Workspace *ws)
     a.E = g.E;
     a.value = ws->value;
     a.dist = reinterpret_cast<unsigned long long *>(ws->value);
-    a.qd = ws->qd;
     a.rcls = ws->rcls;
     a.visited = ws->visited;
     a.front0 = ws->front[0];
