@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched many-graph measurement")
     ap.add_argument("--batched-only", action="store_true", help="run only the batched many-graph measurement")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0, help="target seconds of CPU baseline work")
+    ap.add_argument("--save-tune-table", default=None,
+                    help="write the table of autotuned launch shapes here at the end (a file for weights/)")
     return ap.parse_args()
 
 
@@ -555,6 +557,8 @@ def run_ours(a):
             except Exception as ex:  # a reported baseline, never required for the GPU number
                 line["reference_gpu"] = {"unavailable": f"not run: {ex}"}
         print(json.dumps(line), flush=True)
+        if a.save_tune_table:
+            T.tune_table_save(a.save_tune_table)
     g.free()
     if world > 1:
         dist.barrier()

@@ -17,6 +17,7 @@ constexpr int kFeat = 10;
 constexpr int kHidden = 32;
 constexpr int kBfsOut = 2;      // 0 = top-down (push), 1 = bottom-up (pull)
 constexpr int kSsspOut = 6;     // bucket width = delta * 4^k, k = 0..5 (merge 1 .. 1024 buckets)
+constexpr double kBfsGate = 8.0;  // BFS steps within this factor of a Beamer threshold consult the network
 
 __host__ __device__ constexpr int mlp_param_count(int O)
 {

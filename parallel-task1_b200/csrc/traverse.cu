@@ -539,10 +539,10 @@ struct WarpStage {
 constexpr int kWDefer = 32 + 32 * kBatchSssp;
 // Where a drain takes a candidate's row-class flags from: the gathered
 // distance word, staged with the candidate (0), or the byte array, loaded in
-// parallel with the atomic (1).  Same results either way; the byte frees the
-// registers and shared memory of the staged flags.
+// parallel with the atomic (1).  Same results either way.  Measured on the
+// bench step (128 queries, RMAT s23): 143.0 ms staged, 148.6 ms from the byte.
 #ifndef TRAV_CLS_BYTE
-#define TRAV_CLS_BYTE 1
+#define TRAV_CLS_BYTE 0
 #endif
 struct DeferStage {
     int v[kWDefer];
@@ -1176,9 +1176,15 @@ __device__ __forceinline__ int bfs_query(const TravArgs &a, QueryShared &sh, int
                 plain = 0;
             }
             const Feat f = bfs_features(L, nf, mf, mu, nf_prev, a.V, a.E, prev_dir, plain);
+            // The network is consulted only near Beamer's switching points
+            // (within kBfsGate of either threshold): far from them its answer is
+            // Beamer's, and on long chains of tiny steps (a grid has thousands)
+            // the inference itself would cost more than any choice can save.
+            const bool near = dir == 0 ? (double)mf * a.alpha * kBfsGate > (double)mu
+                                       : (double)nf * a.beta < (double)a.V * kBfsGate;
             int d = plain;
             if (a.force_dir >= 0) d = (L == 0) ? 0 : a.force_dir;
-            else if (a.mlp) d = mlp_argmax_warp<kBfsOut>(sh.mlp, f, plain, a.mlp_margin);
+            else if (a.mlp && near) d = mlp_argmax_warp<kBfsOut>(sh.mlp, f, plain, a.mlp_margin);
             const int forced = planned(a, L);
             if (forced >= 0) d = forced;
             log_decision(ctl, lg, f, d, 0.0f, 0.0f);
