@@ -391,7 +391,7 @@ def run_ours(a):
 
     from pytrav import learn
 
-    have_learned = learn.install(g)  # trained schedule networks shipped in parallel-task1_b200/weights
+    have_learned = learn.install(g, delta=a.delta)  # trained schedule networks shipped in parallel-task1_b200/weights
     schedules = ([T.SCHEDULE_LEARNED] if have_learned else []) + [T.SCHEDULE_PLAIN]
     primary = schedules[0]
     names = {T.SCHEDULE_PLAIN: "plain", T.SCHEDULE_LEARNED: "learned"}

@@ -277,6 +277,18 @@ int trav_pairs_file_read(const char *path, int32_t vertices_pow, int32_t *vertic
  * reference has no learned schedule. */
 int trav_mlp_set(trav_graph *g, int32_t kind, const float *params, int32_t count);
 
+/* The learned schedule's choice of delta for this graph: TRAV_SCHEDULE_LEARNED
+ * SSSP queries (single and batched) on this handle run with delta x scale as
+ * the light/heavy threshold and as the unit of the bucket widths their
+ * network picks; plain queries keep the caller's delta.  scale is chosen per
+ * graph by the learned split model from the graph's degree and weight
+ * statistics (pytrav.learn); default 1.  The distances are the same bits for
+ * every delta.  New. */
+int trav_set_sssp_split(trav_graph *g, float scale);
+
+/* Mean edge weight of a graph (a schedule feature). */
+int trav_graph_mean_weight(const trav_graph *g, float *mean_weight);
+
 /* Abstention margin of the kind's schedule network on this handle: at each
  * decision the network keeps the plain schedule's option (Beamer's direction;
  * delta x 1) unless its best output logit beats that option's logit by at

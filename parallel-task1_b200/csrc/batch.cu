@@ -187,10 +187,11 @@ int build_queries(trav_batch *b, const trav_query *qs, int32_t n, std::vector<Ba
         d.loff = nullptr;
         d.ledge = nullptr;
         if (q.kind == 1 && finite_delta(q.delta)) {
-            d.delta = q.delta;
+            // the learned schedule also picks the query's delta (the graph's learned split)
+            d.delta = d.mlp ? q.delta * g->ws.split_scale : q.delta;
             // light rows once per (graph, delta) for the batch's lifetime
-            LightRows &lr = b->light[std::make_pair(q.graph, q.delta)];
-            TRY(light_rows_build(g->g, q.delta, &lr, b->st));
+            LightRows &lr = b->light[std::make_pair(q.graph, d.delta)];
+            TRY(light_rows_build(g->g, d.delta, &lr, b->st));
             d.nlight = lr.nlight;
             d.loff = lr.loff;
             d.ledge = lr.ledge;

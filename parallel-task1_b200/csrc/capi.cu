@@ -177,6 +177,7 @@ std::vector<unsigned char> capture_key(const trav_graph *g, int kind, const int3
     put(k, g->ws.plan[kind]);
     put(k, g->ws.plan_len[kind]);
     put(k, g->ws.max_steps);
+    put(k, g->ws.split_scale);
     put(k, g->ws.light.nlight);
     put(k, g->ws.light.loff);
     put(k, g->ws.light.ledge);
@@ -231,7 +232,8 @@ int run_batch(trav_graph *g, int kind, const int32_t *sources, int32_t n, const 
         // the light rows of delta are built before the capture (it allocates
         // and synchronises); the graph bakes in their addresses, which are part
         // of the key, so a rebuild for another delta records a new graph
-        if (kind == 1 && delta > 0.0f && std::isfinite(delta)) TRY(light_rows_build(g->g, delta, &g->ws.light, g->st));
+        if (kind == 1 && delta > 0.0f && std::isfinite(delta))
+            TRY(light_rows_build(g->g, mlp ? delta * g->ws.split_scale : delta, &g->ws.light, g->st));
         std::vector<unsigned char> key = capture_key(g, kind, sources, n, bo, delta, mlp, out);
         if (!c.exec || c.key != key) {
             if (c.exec) cudaGraphExecDestroy(c.exec);
@@ -384,6 +386,23 @@ int trav_graph_info(const trav_graph *g, int32_t *vertices, int64_t *edges, int3
     if (vertices) *vertices = g->g.V;
     if (edges) *edges = g->g.E;
     if (max_out_degree) *max_out_degree = g->g.max_out_degree;
+    return TRAV_OK;
+}
+
+int trav_graph_mean_weight(const trav_graph *g, float *mean_weight)
+{
+    if (!g || !mean_weight) return bad("graph handle and mean_weight must not be NULL");
+    *mean_weight = g->g.mean_w;
+    return TRAV_OK;
+}
+
+int trav_set_sssp_split(trav_graph *g, float scale)
+{
+    if (!g) return bad("graph handle is NULL");
+    if (!(scale > 0.0f) || !std::isfinite(scale)) return bad("scale must be finite and > 0");
+    TRY_CUDA(cudaSetDevice(g->device));
+    TRY_CUDA(cudaStreamSynchronize(g->st));
+    g->ws.split_scale = scale;
     return TRAV_OK;
 }
 

@@ -138,6 +138,7 @@ struct Workspace {
     int item = kItem;
     int max_steps = 0;                 // step budget of a query; 0 = the default (see launch_bfs / launch_sssp)
     float mlp_margin[2] = {0.0f, 0.0f};  // abstention margins of the BFS / SSSP networks
+    float split_scale = 1.0f;          // learned SSSP queries run with delta x split_scale (the learned split)
     unsigned long long timeout_ns = 0;  // bounded wait of a grid barrier; 0 = kDefaultTimeoutNs
 };
 

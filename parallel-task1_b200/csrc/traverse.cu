@@ -2109,6 +2109,9 @@ int launch_sssp(const DevGraph &g, Workspace *ws, int q, int32_t source_new, flo
     if (ws->max_steps > 0 && ws->max_steps < a.max_steps) a.max_steps = ws->max_steps;
     a.force_dir = -1;
     a.delta = (delta > 0.0f && std::isfinite(delta)) ? delta : INFINITY;
+    // the learned schedule also picks the query's delta: its split scales the
+    // caller's delta (light/heavy threshold and the unit of the bucket widths)
+    if (mlp && std::isfinite(a.delta)) a.delta *= ws->split_scale;
     if (source_new < 0) {
         // start from distance bits gathered into the second queue buffer (read
         // by the initialisation only); every edge is light there

@@ -54,6 +54,7 @@ EXPORTS = [
     "trav_el_optimize", "trav_el_gpu_transactions", "trav_adj_file_read", "trav_adj_file_write",
     "trav_pairs_file_read", "trav_set_limits", "trav_inject_alloc_failure", "trav_reach_el_masked",
     "trav_mlp_set_margin", "trav_batch_run_host", "trav_tune_table_save", "trav_tune_table_load",
+    "trav_set_sssp_split", "trav_graph_mean_weight",
 ]
 
 
@@ -122,6 +123,8 @@ def lib():
         L.trav_pairs_file_read.argtypes = [C.c_char_p, i32, C.POINTER(i32), C.POINTER(i64), vp, vp, vp]
         L.trav_mlp_set.argtypes = [vp, i32, vp, i32]
         L.trav_mlp_set_margin.argtypes = [vp, i32, f32]
+        L.trav_set_sssp_split.argtypes = [vp, f32]
+        L.trav_graph_mean_weight.argtypes = [vp, C.POINTER(f32)]
         L.trav_set_grid.argtypes = [vp, i32, i32, C.POINTER(i32)]
         L.trav_graph_set_capture.argtypes = [vp, i32]
         L.trav_el_optimize.argtypes = [vp, vp, vp, i32, i64, i32, i32, C.POINTER(i64)]
@@ -332,6 +335,16 @@ class Graph:
     def set_mlp(self, kind: int, params):
         p = np.ascontiguousarray(params, np.float32)
         _check(lib().trav_mlp_set(self._h, kind, p.ctypes.data, len(p)))
+
+    def set_sssp_split(self, scale: float):
+        """Learned SSSP queries on this graph run with delta x scale (the learned split; 1 = the caller's delta)."""
+        _check(lib().trav_set_sssp_split(self._h, float(scale)))
+
+    @property
+    def mean_weight(self) -> float:
+        w = C.c_float(0.0)
+        _check(lib().trav_graph_mean_weight(self._h, C.byref(w)))
+        return w.value
 
     def set_mlp_margin(self, kind: int, margin: float):
         """Logit margin the kind's network needs to leave the plain option (0 = plain argmax)."""
