@@ -503,6 +503,11 @@ __device__ void write_back(const TravArgs &a)
 #ifndef TRAV_LIGHT_ROWS
 #define TRAV_LIGHT_ROWS 1
 #endif
+// Pull rounds stage one candidate per owner and batch, the min of a warp
+// segment (1), or every improving in-edge (0); both give the same results.
+#ifndef TRAV_PULL_REDUCE
+#define TRAV_PULL_REDUCE 1
+#endif
 #ifndef TRAV_FLUSH_ATTR
 #define TRAV_FLUSH_ATTR __forceinline__
 #endif
@@ -977,6 +982,39 @@ struct SsspVisit {
 #pragma unroll
             for (int j = 0; j < kBatch; j++) nd[j] = ok[j] ? dist_of(ld_gather(&a->dist[v[j]])) : 0.0f;
             DeferStage *d = p.d;
+#if TRAV_PULL_REDUCE
+            // Lane k of batch j holds edge base + 32 j + k, so for each j the
+            // lanes of one owner are contiguous.  A segmented min leaves an
+            // owner's best candidate at its first lane, and only that lane
+            // stages it: one atomic per owner and batch instead of one per
+            // improving in-edge (the owner is unsettled, so most of its
+            // in-edges improve on its distance at the round's start).  The
+            // candidates are >= +0, so their bits order as unsigned integers.
+            const unsigned lane = lane_id();
+#pragma unroll
+            for (int j = 0; j < kBatch; j++) {
+                nd[j] = __fadd_rn(nd[j], w[j]);  // one rounded add, as sssp.hpp:56
+                const int o = ok[j] ? us[j] : -1;
+                const int prev = __shfl_up_sync(kFull, o, 1);
+                const unsigned heads = __ballot_sync(kFull, lane == 0 || prev != o);
+                const unsigned later = heads & ~((2u << lane) - 1u);  // heads above this lane (none for lane 31)
+                const unsigned end = later ? (unsigned)__ffs(later) - 1u : 32u;  // first lane past this segment
+                unsigned key = ok[j] && nd[j] < du[j] ? __float_as_uint(nd[j]) : 0xffffffffu;
+#pragma unroll
+                for (unsigned s = 1; s < 32; s <<= 1) {
+                    const unsigned y = __shfl_down_sync(kFull, key, s);
+                    if (lane + s < end) key = min(key, y);
+                }
+                const bool cand = (heads >> lane & 1u) && key != 0xffffffffu;
+                const unsigned m = __ballot_sync(kFull, cand);
+                if (cand) {
+                    const unsigned i = p.ndef + __popc(m & lanemask_lt());
+                    d->v[i] = us[j];
+                    d->d[i] = __uint_as_float(key);
+                }
+                p.ndef += __popc(m);
+            }
+#else
 #pragma unroll
             for (int j = 0; j < kBatch; j++) {
                 nd[j] = __fadd_rn(nd[j], w[j]);  // one rounded add, as sssp.hpp:56
@@ -989,6 +1027,7 @@ struct SsspVisit {
                 }
                 p.ndef += __popc(m);
             }
+#endif
             while (p.ndef >= 32) drain(p, 32);
         } else {
             load_at<kPart>(e, ok, v, w);
