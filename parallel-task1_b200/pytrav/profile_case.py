@@ -1,5 +1,6 @@
-"""A small, fixed traversal workload to put under a profiler: the bench's RMAT graph (a=0.57, b=c=0.19, seed 1,
-self loops dropped) at a chosen scale, n seeded sources picked as the bench picks them, the learned schedule.
+"""A small, fixed traversal workload to put under a profiler: the bench's RMAT graph (a/b/c/d 57/19/19/5
+percent, seed 1, self loops dropped) at a chosen scale, n seeded sources picked as the bench picks them, and the
+learned schedule.
 
     python -m pytrav.profile_case --scale 22 --sources 8 --mode batch
 
@@ -16,7 +17,7 @@ import sys
 
 import numpy as np
 
-ABCD = (0.57, 0.19, 0.19, 0.05)
+ABCD = (57, 19, 19, 5)  # integer percents, as the reference generator takes them
 
 
 def pick_sources(deg, n, seed):
