@@ -93,9 +93,9 @@ TeamLayout team_layout(const trav_batch *b)
     return L;
 }
 
-int ensure_teams(trav_batch *b, int teams)
+// Free the team scratch (run_launch allocates it again, sized to what is free).
+int release_teams(trav_batch *b)
 {
-    if (teams <= b->teams_alloc) return TRAV_OK;
     TRY_CUDA(cudaStreamSynchronize(b->st));
     cudaFree(b->team_mem);
     cudaFree(b->d_teams);
@@ -104,6 +104,13 @@ int ensure_teams(trav_batch *b, int teams)
     b->d_teams = nullptr;
     b->ctl = nullptr;
     b->teams_alloc = 0;
+    return TRAV_OK;
+}
+
+int ensure_teams(trav_batch *b, int teams)
+{
+    if (teams <= b->teams_alloc) return TRAV_OK;
+    TRY(release_teams(b));
     const TeamLayout L = team_layout(b);
     b->team_bytes = L.total;
     TRY_CUDA(dev_malloc(&b->team_mem, L.total * (size_t)teams));
@@ -413,6 +420,10 @@ int trav_batch_run_host(trav_batch *b, const trav_query *queries, int32_t n, int
         cudaFree(b->staging);
         b->staging = nullptr;
         b->staging_bytes = 0;
+        // Team scratch is sized to the free memory when it is allocated, so on
+        // a large graph it may have left too little for the staging area:
+        // place the staging first and let the launches size the teams again.
+        TRY(release_teams(b));
         TRY_CUDA(dev_malloc(&b->staging, at[(size_t)n]));
         b->staging_bytes = at[(size_t)n];
     }

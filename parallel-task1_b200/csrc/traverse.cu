@@ -508,6 +508,13 @@ __device__ void write_back(const TravArgs &a)
 #ifndef TRAV_PULL_REDUCE
 #define TRAV_PULL_REDUCE 1
 #endif
+// BFS bottom-up steps count the vertices they find and leave them in the
+// frontier bitmap only; a top-down step that follows builds its queue from
+// that bitmap in one extra phase (1).  Or every bottom-up step pushes its
+// found vertices to the queue as it goes (0).  Both give the same levels.
+#ifndef TRAV_BU_LAZY
+#define TRAV_BU_LAZY 1
+#endif
 #ifndef TRAV_FLUSH_ATTR
 #define TRAV_FLUSH_ATTR __forceinline__
 #endif
@@ -1248,6 +1255,29 @@ __device__ __forceinline__ int bfs_query(const TravArgs &a, QueryShared &sh, int
             log_phase(ctl, lg, 2, (unsigned)nf);
             ph++;
         }
+#if TRAV_BU_LAZY
+        if (dir == 0 && prev_dir == 1) {
+            // frontier queue from the bitmap of the vertices the last
+            // bottom-up step found (bottom-up steps push nothing)
+            clear_ahead(a, ph);
+            const FrontierOut qo{{(cur ? a.q1 : a.q0), nullptr}, {(cur ? a.chunks1 : a.chunks0), nullptr}, {0u, 0u},
+                                 {0u, 0u}, {kPartWhole, kPartWhole}, nullptr, 0u, &ctl->slot[ph % kSlots]};
+            Pusher pq = make_pusher(a, qo, mys);
+            const unsigned *fc = fcur ? a.front1 : a.front0;
+            for (unsigned w = gwarp; w < (unsigned)a.W; w += nwarps) {
+                const int v = (int)(w * 32 + lane_id());
+                const bool f = v < a.V && ((fc[w] >> lane_id()) & 1u);
+                const unsigned deg = f ? (unsigned)(__ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v])) : 0u;
+                push(pq, 0, f, v, deg);
+            }
+            finish_phase(pq, cc);
+            if (!grid_sync(a, ph, &s_view)) return -1;
+            log_phase(ctl, lg, 2, (unsigned)nf);
+            nq = s_view.q_add;
+            nch = s_view.chunk_add;
+            ph++;
+        }
+#endif
         clear_ahead(a, ph);
         const FrontierOut out{{(cur ? a.q0 : a.q1), nullptr}, {(cur ? a.chunks0 : a.chunks1), nullptr}, {0u, 0u},
                               {0u, 0u}, {kPartWhole, kPartWhole}, nullptr, 0u, &ctl->slot[ph % kSlots]};
@@ -1318,7 +1348,13 @@ __device__ __forceinline__ int bfs_query(const TravArgs &a, QueryShared &sh, int
                     deg = (unsigned)(__ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v]));
                 }
                 p.mf += deg;
+#if TRAV_BU_LAZY
+                // the found vertices are counted (in the slot's hbig_add, which
+                // BFS leaves unused) and queued only if a top-down step follows
+                p.big_total[1] += __popc(m);
+#else
                 push(p, 0, found, v, deg);
+#endif
             }
             fcur ^= 1;
             bu_steps++;
@@ -1333,7 +1369,8 @@ __device__ __forceinline__ int bfs_query(const TravArgs &a, QueryShared &sh, int
         nch = s0.chunk_add;
         mu -= s0.mf;
         nf_prev = nf;
-        nf = (unsigned long long)s0.q_add + s0.big_add;
+        nf = TRAV_BU_LAZY && dir == 1 ? (unsigned long long)s0.hbig_add
+                                      : (unsigned long long)s0.q_add + s0.big_add;
         mf = s0.mf;
         prev_dir = dir;
         L++;

@@ -7,7 +7,7 @@ learned schedule.
 Modes:
   batch  two launches of one batch_persistent kernel over the n BFS and n SSSP queries, at a fixed launch shape
          (so no autotuner trials run first); capture the second with `-k regex:batch_persistent -s 1 -c 1`;
-  sssp   the n SSSP queries twice as single-query sssp_persistent launches (capture with `-s <n> -c 1`);
+  sssp   the n SSSP queries twice as single-query sssp_persistent launches (capture with `-s <2n> -c 1`);
   bfs    the same for bfs_persistent.
 
 The graph, its light rows and the outputs are all the device holds: about 2.5 GB at scale 22 and 5 GB at 23."""
@@ -49,6 +49,16 @@ def main(argv=None):
     n, V = len(srcs), g.V
     lv = torch.empty((n, V), dtype=torch.int32, device="cuda")
     di = torch.empty((n, V), dtype=torch.float32, device="cuda")
+    # algorithmic bytes of the queries (one single-query launch each; the count is the same however a query runs)
+    alg = 0
+    for i, s in enumerate(srcs):
+        if a.mode in ("batch", "bfs"):
+            g.bfs([s], out=lv[i:i + 1], schedule=T.SCHEDULE_LEARNED)
+            alg += g.last_stats().algorithmic_bytes
+        if a.mode in ("batch", "sssp"):
+            g.sssp([s], out=di[i:i + 1], delta=a.delta, schedule=T.SCHEDULE_LEARNED)
+            alg += g.last_stats().algorithmic_bytes
+    print(f"algorithmic bytes of the {a.mode} queries: {alg}")
     if a.mode == "batch":
         b = T.Batch([g])
         b.shape = tuple(int(x) for x in a.shape.split(","))
