@@ -241,6 +241,7 @@ struct BatchArgs {
     unsigned int *next;         // dispatch counter, zero at launch
     const TeamWs *teams;
     int32_t team_ctas;          // CTAs per team; the launch has a whole number of teams
+    int32_t full_ctas;          // co-resident CTAs of the device (a single query's grid)
     int32_t small_deg, item;
     unsigned long long timeout_ns;
 };

@@ -515,6 +515,17 @@ __device__ void write_back(const TravArgs &a)
 #ifndef TRAV_BU_LAZY
 #define TRAV_BU_LAZY 1
 #endif
+// Bitmap words a warp works on at once in a bottom-up step.
+#ifndef TRAV_BU_WORDS
+#define TRAV_BU_WORDS 3
+#endif
+constexpr int kBuWords = TRAV_BU_WORDS;
+// In-rows longer than this are scanned by the whole warp in a bottom-up step;
+// shorter ones by their own lane, four parents per probe.
+#ifndef TRAV_BU_COOP
+#define TRAV_BU_COOP 512
+#endif
+constexpr int kBuCoop = TRAV_BU_COOP;
 #ifndef TRAV_FLUSH_ATTR
 #define TRAV_FLUSH_ATTR __forceinline__
 #endif
@@ -1286,75 +1297,109 @@ __device__ __forceinline__ int bfs_query(const TravArgs &a, QueryShared &sh, int
             const BfsPush vis{&a, L + 1};
             expand_frontier<kPartWhole>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, p);
         } else {
-            // bottom-up: each warp owns 32 vertices = one bitmap word
+            // bottom-up: each warp owns 32 vertices = one bitmap word, and works
+            // on kBuWords words at once (w, w + nwarps, ...) so that the
+            // dependent loads of one word (visited -> in_off -> in_adj ->
+            // frontier bit) overlap those of the others
             const unsigned *fc = fcur ? a.front1 : a.front0;
             unsigned *fn = fcur ? a.front0 : a.front1;
-            for (unsigned w = gwarp; w < (unsigned)a.W; w += nwarps) {
-                // The frontier bitmap and this word of `visited` were written in
-                // earlier phases and only this warp writes the word now: plain
+            constexpr int kW = kBuWords;
+            const int lane = (int)lane_id();
+            for (unsigned w0 = gwarp; w0 < (unsigned)a.W; w0 += kW * nwarps) {
+                // The frontier bitmap and these words of `visited` were written
+                // in earlier phases and only this warp writes them now: plain
                 // (L1-cacheable) loads are coherent after the grid barrier.
-                const int lane = (int)lane_id();
-                const int v = (int)(w * 32 + lane);
-                const unsigned vis = a.visited[w];
-                bool cand = v < a.V && !((vis >> lane) & 1u);
-                int k = 0, kend = 0;
-                if (cand) {
-                    k = __ldg(&a.in_off[v]);
-                    kend = __ldg(&a.in_off[v + 1]);
+                unsigned wd[kW], vis[kW];
+                bool live[kW], cand[kW], found[kW];
+                int v[kW], k[kW], kend[kW];
+#pragma unroll
+                for (int i = 0; i < kW; i++) {
+                    wd[i] = w0 + (unsigned)i * nwarps;
+                    live[i] = wd[i] < (unsigned)a.W;
+                    vis[i] = live[i] ? a.visited[wd[i]] : ~0u;
+                    v[i] = (int)(wd[i] * 32 + lane);
                 }
-                bool found = false;
+#pragma unroll
+                for (int i = 0; i < kW; i++) {
+                    cand[i] = live[i] && v[i] < a.V && !((vis[i] >> lane) & 1u);
+                    found[i] = false;
+                    k[i] = kend[i] = 0;
+                    if (cand[i]) {
+                        k[i] = __ldg(&a.in_off[v[i]]);
+                        kend[i] = __ldg(&a.in_off[v[i] + 1]);
+                    }
+                }
                 // long in-rows: the whole warp scans one row 32 entries at a time
-                unsigned coop = __ballot_sync(kFull, cand && kend - k > 32);
-                while (coop) {
-                    const int owner = __ffs(coop) - 1;
-                    coop &= coop - 1;
-                    const int kb = __shfl_sync(kFull, k, owner), ke = __shfl_sync(kFull, kend, owner);
-                    bool hit = false;
-                    for (int kk = kb + lane; kk - lane < ke; kk += 32) {
-                        bool h = false;
-                        if (kk < ke) {
-                            const int u = ld_stream(&a.in_adj[kk]);
-                            h = (fc[u >> 5] >> (u & 31)) & 1u;
-                        }
-                        if (__any_sync(kFull, h)) {
-                            hit = true;
-                            break;
-                        }
-                    }
-                    if (lane == owner) {
-                        found = hit;
-                        cand = false;
-                    }
-                }
-                // short in-rows: one lane each, four parents per probe (independent loads)
-                if (cand) {
-                    for (; k < kend && !found; k += 4) {
-                        int u[4];
 #pragma unroll
-                        for (int i = 0; i < 4; i++) u[i] = k + i < kend ? ld_stream(&a.in_adj[k + i]) : -1;
-#pragma unroll
-                        for (int i = 0; i < 4; i++)
-                            if (u[i] >= 0 && ((fc[u[i] >> 5] >> (u[i] & 31)) & 1u)) found = true;
+                for (int i = 0; i < kW; i++) {
+                    unsigned coop = __ballot_sync(kFull, cand[i] && kend[i] - k[i] > kBuCoop);
+                    while (coop) {
+                        const int owner = __ffs(coop) - 1;
+                        coop &= coop - 1;
+                        const int kb = __shfl_sync(kFull, k[i], owner), ke = __shfl_sync(kFull, kend[i], owner);
+                        bool hit = false;
+                        for (int kk = kb + lane; kk - lane < ke; kk += 32) {
+                            bool h = false;
+                            if (kk < ke) {
+                                const int u = ld_stream(&a.in_adj[kk]);
+                                h = (fc[u >> 5] >> (u & 31)) & 1u;
+                            }
+                            if (__any_sync(kFull, h)) {
+                                hit = true;
+                                break;
+                            }
+                        }
+                        if (lane == owner) {
+                            found[i] = hit;
+                            cand[i] = false;
+                        }
                     }
                 }
-                const unsigned m = __ballot_sync(kFull, found);
-                if (lane == 0) {
-                    fn[w] = m;
-                    if (m) a.visited[w] = vis | m;
+                // short in-rows: one lane each, four parents per row and probe
+                // (the probes of the lane's kW rows are independent loads)
+                for (;;) {
+                    bool act[kW], any = false;
+#pragma unroll
+                    for (int i = 0; i < kW; i++) {
+                        act[i] = cand[i] && !found[i] && k[i] < kend[i];
+                        any |= act[i];
+                    }
+                    if (!any) break;
+                    int u[kW][4];
+#pragma unroll
+                    for (int i = 0; i < kW; i++)
+#pragma unroll
+                        for (int j = 0; j < 4; j++) u[i][j] = act[i] && k[i] + j < kend[i] ? ld_stream(&a.in_adj[k[i] + j]) : -1;
+#pragma unroll
+                    for (int i = 0; i < kW; i++) {
+#pragma unroll
+                        for (int j = 0; j < 4; j++)
+                            if (u[i][j] >= 0 && ((fc[u[i][j] >> 5] >> (u[i][j] & 31)) & 1u)) found[i] = true;
+                        k[i] += 4;
+                    }
                 }
-                unsigned deg = 0;
-                if (found) {
-                    reinterpret_cast<int *>(a.value)[v] = L + 1;
-                    deg = (unsigned)(__ldg(&a.out_off[v + 1]) - __ldg(&a.out_off[v]));
-                }
-                p.mf += deg;
+#pragma unroll
+                for (int i = 0; i < kW; i++) {
+                    const unsigned m = __ballot_sync(kFull, found[i]);
+                    if (lane == 0 && live[i]) {
+                        fn[wd[i]] = m;
+                        if (m) a.visited[wd[i]] = vis[i] | m;
+                    }
+                    unsigned deg = 0;
+                    if (found[i]) {
+                        reinterpret_cast<int *>(a.value)[v[i]] = L + 1;
+                        deg = (unsigned)(__ldg(&a.out_off[v[i] + 1]) - __ldg(&a.out_off[v[i]]));
+                    }
+                    p.mf += deg;
 #if TRAV_BU_LAZY
-                // the found vertices are counted (in the slot's hbig_add, which
-                // BFS leaves unused) and queued only if a top-down step follows
-                p.big_total[1] += __popc(m);
+                    // the found vertices are counted (in the slot's hbig_add,
+                    // which BFS leaves unused) and queued only if a top-down
+                    // step follows
+                    p.big_total[1] += __popc(m);
 #else
-                push(p, 0, found, v, deg);
+                    push(p, 0, found[i], v[i], deg);
 #endif
+                }
             }
             fcur ^= 1;
             bu_steps++;
@@ -1759,6 +1804,13 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) batch_persistent
             a.max_steps = q.V + 1;
             a.alpha = 15.0f;
             a.beta = 18.0f;
+            // The direction network was trained on queries that own the whole
+            // grid.  A bottom-up step scans every unvisited vertex, so on a team
+            // of a fraction of the grid it costs that much more against a
+            // top-down step than the network saw: there a learned query keeps
+            // Beamer's switch (on 74-CTA teams at RMAT s23 the network's
+            // directions ran 10% slower than Beamer's; on the full grid, even).
+            if (2 * b.team_ctas <= b.full_ctas) a.mlp = nullptr;
             a.force_dir = -1;
             a.delta = 0.0f;
             a.out_kind = 0;
@@ -2039,6 +2091,7 @@ int launch_batch(BatchArgs b, int teams, cudaStream_t st, cudaEvent_t ev0, cudaE
         set_error("batch launch shape exceeds the co-resident CTAs");
         return TRAV_ERR_BAD_ARG;
     }
+    b.full_ctas = most;
     TRY_CUDA(cudaMemsetAsync(b.next, 0, sizeof(unsigned), st));
     if (ev0) TRY_CUDA(cudaEventRecord(ev0, st));
     void *params[] = {&b};
