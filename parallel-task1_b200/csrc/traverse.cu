@@ -543,9 +543,13 @@ constexpr int kWFarFlush = 128, kWFar = kWFarFlush + 32;
 
 constexpr int kPartWhole = 0, kPartLight = 1, kPartHeavy = 2, kPartIn = 3;  // kPartIn: the in-row (CSC)
 // An SSSP heavy round considers pulling when its heavy list may hold more than
-// 1/kPullCheck of the graph's edges.
+// 1/kPullCheck of the graph's edges.  The check is a pass over every vertex,
+// which a query on a batch team of 1/8 of the grid pays eight times over:
+// summed over four graphs (RMAT s23 ef32, s24 ef16, a flatter RMAT, uniform
+// 2^23), 64-query SSSP batches took 854 ms at 3, 864 at 4 and 871 at 8, and
+// single queries were also fastest at 3.
 #ifndef TRAV_PULL_CHECK
-#define TRAV_PULL_CHECK 8.0
+#define TRAV_PULL_CHECK 3.0
 #endif
 constexpr double kPullCheck = TRAV_PULL_CHECK;
 
