@@ -421,17 +421,18 @@ void trav_batch_free(trav_batch *b);
 int trav_batch_run(trav_batch *b, const trav_query *queries, int32_t n, float *device_ms);
 
 /* The same queries with HOST output arrays (`out` = V results in host
- * memory; pinned memory lets the copies overlap the work).  The queries run
- * as `parts` launches over consecutive slices of the array, slices shrinking
- * in the ratio 2 (parts - p) + 1; each slice's results are staged in device
- * memory and copied to the host on a second stream while the next slice
- * runs, so only the small last slice's copy follows the last launch.  Put
- * mixed kinds side by side in the array (e.g. the BFS and SSSP queries of one
- * source next to each other) so the slices balance.  *device_ms (may be
- * NULL) receives the summed device time of the launches.  Returns after the
- * last copy has finished.  The reference's counterpart is the per-call
- * upload / kernel / copy-back of gpu_bellman_ford (algorithm/sssp/
- * sssp.hpp:219-277). */
+ * memory; pinned memory lets the copies overlap the work).  Each query's
+ * results are staged in device memory; the kernel raises a completion flag in
+ * mapped host memory once a query's team has written them all, and the
+ * calling thread, polling the flags while the launch runs, copies that
+ * query's results to the host on a second stream.  So the copies overlap the
+ * remaining queries and only the last ones follow the launch.  The queries
+ * run as `parts` launches over consecutive slices of the array (slices
+ * shrinking in the ratio 2 (parts - p) + 1); parts = 1 is normally fastest.
+ * *device_ms (may be NULL) receives the summed device time of the launches.
+ * Returns after the last copy has finished.  The reference's counterpart is
+ * the per-call upload / kernel / copy-back of gpu_bellman_ford
+ * (algorithm/sssp/sssp.hpp:219-277). */
 int trav_batch_run_host(trav_batch *b, const trav_query *queries, int32_t n, int32_t parts, float *device_ms);
 
 /* Process-wide table of the launch shapes the autotuner found, keyed by the

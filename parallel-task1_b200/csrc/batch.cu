@@ -8,10 +8,13 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -54,7 +57,8 @@ struct trav_batch {
     unsigned char *staging = nullptr;
     size_t staging_bytes = 0;
     cudaStream_t cst = nullptr;
-    cudaEvent_t part_done = nullptr;
+    unsigned *done = nullptr;  // per-query completion flags, mapped host memory
+    int done_cap = 0;
     trav_batch_shape shape{16, kSmallDeg, kItem};
 };
 
@@ -156,6 +160,8 @@ int shape_ok(const trav_batch_shape &s, int most)
 
 bool finite_delta(float d) { return d > 0.0f && std::isfinite(d); }
 
+constexpr int kBusy = 1;  // a run_launch poll's "keep calling me" (TRAV_OK and the errors are <= 0)
+
 // Descriptors in dispatch order: the most edges first (an SSSP query counts
 // as four BFS queries), so the long queries start while the short ones fill
 // the gaps.
@@ -185,6 +191,7 @@ int build_queries(trav_batch *b, const trav_query *qs, int32_t n, std::vector<Ba
         d.mean_w = g->g.mean_w;
         d.max_deg = g->g.max_out_degree;
         d.kind = q.kind;
+        d.id = i;
         d.source = g->new_of_old[(size_t)q.source];
         d.out = q.out;
         d.mlp = q.schedule == TRAV_SCHEDULE_LEARNED ? g->mlp[q.kind] : nullptr;
@@ -231,7 +238,11 @@ int check_queries_host(const trav_batch *b, const trav_query *qs, int32_t n)
 namespace {
 
 // One launch of the queries already in b->d_q; *ms receives its device time.
-int run_launch(trav_batch *b, int32_t n, const trav_batch_shape &s, float *ms)
+// `done` (mapped host flags, may be nullptr) is passed to the kernel; while the
+// launch runs, `poll` (may be empty) is called until it returns something other
+// than kBusy or the launch has ended.
+int run_launch(trav_batch *b, int32_t n, const trav_batch_shape &s, float *ms, unsigned *done = nullptr,
+               const std::function<int(bool ended)> &poll = {})
 {
     const int most = persistent_grid_size(2);
     if (most <= 0) return TRAV_ERR_CUDA;
@@ -263,9 +274,21 @@ int run_launch(trav_batch *b, int32_t n, const trav_batch_shape &s, float *ms)
     a.small_deg = s.small_deg;
     a.item = s.item;
     a.timeout_ns = 10ull * 1000000000ull;
+    a.done = done;
     TRY(launch_batch(a, teams, b->st, b->ev0, b->ev1));
+    int prc = TRAV_OK;
+    if (poll) {
+        // the kernel's own barrier waits are bounded, so the launch ends and so does this loop
+        for (;;) {
+            const bool ended = cudaStreamQuery(b->st) != cudaErrorNotReady;
+            prc = poll(ended);
+            if (prc != kBusy || ended) break;
+            std::this_thread::yield();
+        }
+    }
     TRY_CUDA(cudaStreamSynchronize(b->st));
     TRY(check_ctls(b->ctl, teams, "batch"));
+    if (prc != TRAV_OK && prc != kBusy) return prc;
     float t = 0.0f;
     TRY_CUDA(cudaEventElapsedTime(&t, b->ev0, b->ev1));
     if (ms) *ms = t;
@@ -378,7 +401,7 @@ void trav_batch_free(trav_batch *b)
     for (auto &kv : b->light) light_rows_free(&kv.second);
     if (b->cst) cudaStreamSynchronize(b->cst);
     cudaFree(b->staging);
-    if (b->part_done) cudaEventDestroy(b->part_done);
+    cudaFreeHost(b->done);
     if (b->cst) cudaStreamDestroy(b->cst);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
@@ -428,12 +451,23 @@ int trav_batch_run_host(trav_batch *b, const trav_query *queries, int32_t n, int
         b->staging_bytes = at[(size_t)n];
     }
     if (!b->cst) TRY_CUDA(cudaStreamCreateWithFlags(&b->cst, cudaStreamNonBlocking));
-    if (!b->part_done) TRY_CUDA(cudaEventCreateWithFlags(&b->part_done, cudaEventDisableTiming));
+    if (n > b->done_cap) {
+        cudaFreeHost(b->done);
+        b->done = nullptr;
+        b->done_cap = 0;
+        TRY_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&b->done), sizeof(unsigned) * (size_t)n, cudaHostAllocMapped));
+        b->done_cap = n;
+    }
+    unsigned *done_dev = nullptr;
+    TRY_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&done_dev), b->done, 0));
     std::vector<trav_query> dq(queries, queries + n);
     for (int32_t i = 0; i < n; i++) dq[(size_t)i].out = b->staging + at[(size_t)i];
-    // Part p holds a share of the queries proportional to 2 (parts - p) + 1: the
-    // parts shrink, so each part's copy (about 0.4 of its compute at RMAT s23)
-    // ends inside the next part's launch and only a small last copy is left.
+    // Part p holds a share of the queries proportional to 2 (parts - p) + 1.
+    // Within a part, each query's results go to the host as soon as its team
+    // has written them: the kernel raises the query's flag in mapped host
+    // memory, and this thread, polling the flags while the launch runs, queues
+    // the copy on a second stream.  Only the last queries' copies follow the
+    // launch, so parts = 1 (one launch) is normally best.
     std::vector<int32_t> cut((size_t)parts + 1, 0);
     double wsum = 0.0;
     for (int p = 0; p < parts; p++) wsum += 2.0 * (parts - p) + 1.0;
@@ -443,20 +477,35 @@ int trav_batch_run_host(trav_batch *b, const trav_query *queries, int32_t n, int
         cut[(size_t)p + 1] = (int32_t)std::lround(n * acc / wsum);
     }
     cut[(size_t)parts] = n;
+    volatile unsigned *flag = b->done;
+    std::vector<char> sent((size_t)n, 0);
+    auto send = [&](int32_t i) -> int {
+        sent[(size_t)i] = 1;
+        TRY_CUDA(cudaMemcpyAsync(queries[i].out, b->staging + at[(size_t)i], at[(size_t)i + 1] - at[(size_t)i],
+                                 cudaMemcpyDeviceToHost, b->cst));
+        return TRAV_OK;
+    };
     float total = 0.0f;
     for (int p = 0; p < parts; p++) {
         const int32_t q0 = cut[(size_t)p], q1 = cut[(size_t)p + 1];
         if (q1 <= q0) continue;
         TRY(upload_queries(b, dq.data() + q0, q1 - q0));
+        std::memset(b->done, 0, sizeof(unsigned) * (size_t)(q1 - q0));
+        int32_t left = q1 - q0;
+        auto poll = [&](bool) -> int {
+            for (int32_t i = q0; i < q1 && left > 0; i++)
+                if (!sent[(size_t)i] && flag[i - q0]) {
+                    TRY(send(i));
+                    left--;
+                }
+            return left > 0 ? kBusy : TRAV_OK;
+        };
         float ms = 0.0f;
-        TRY(run_launch(b, q1 - q0, b->shape, &ms));
+        TRY(run_launch(b, q1 - q0, b->shape, &ms, done_dev, poll));
         total += ms;
-        // the results of this part go to the host while the next part runs
-        TRY_CUDA(cudaEventRecord(b->part_done, b->st));
-        TRY_CUDA(cudaStreamWaitEvent(b->cst, b->part_done, 0));
+        // the launch has ended: whatever was not copied yet goes now
         for (int32_t i = q0; i < q1; i++)
-            TRY_CUDA(cudaMemcpyAsync(queries[i].out, b->staging + at[(size_t)i], at[(size_t)i + 1] - at[(size_t)i],
-                                     cudaMemcpyDeviceToHost, b->cst));
+            if (!sent[(size_t)i]) TRY(send(i));
     }
     TRY_CUDA(cudaStreamSynchronize(b->cst));
     if (device_ms) *device_ms = total;

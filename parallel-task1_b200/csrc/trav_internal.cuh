@@ -223,6 +223,7 @@ struct BatchQuery {
     float delta;            // SSSP bucket width (+inf = Bellman-Ford)
     float mean_w;           // mean edge weight
     int32_t max_deg;        // largest out-degree
+    int32_t id;             // position in the caller's query array (its completion flag)
 };
 
 // Scratch of one team of a batch launch, sized for the batch's largest graph.
@@ -244,6 +245,9 @@ struct BatchArgs {
     int32_t full_ctas;          // co-resident CTAs of the device (a single query's grid)
     int32_t small_deg, item;
     unsigned long long timeout_ns;
+    // completion flags in mapped host memory, one per query by BatchQuery::id
+    // (nullptr = none): set once the query's results are all written
+    unsigned *done;
 };
 
 __device__ __forceinline__ int team_tid(const TravArgs &a) { return (int)(blockIdx.x - a.cta0) * kBlock + (int)threadIdx.x; }

@@ -1755,13 +1755,19 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) batch_persistent
     t.cta0 = team * b.team_ctas;
     t.ctas = b.team_ctas;
     const bool leader = (int)blockIdx.x == t.cta0 && threadIdx.x == 0;
-    int ph = 0;
+    int ph = 0, prev_id = -1;
     while (true) {
         // dispatch phase: the team's first thread takes the next query
         clear_ahead(t, ph);
         if (leader) w.ctl->cur_query = (int)atomicAdd(b.next, 1u);
         if (!grid_sync(t, ph)) return;
         ph++;
+        // every CTA of the team has written (and fenced) its part of the
+        // previous query's results: raise its completion flag for the host
+        if (leader && b.done && prev_id >= 0) {
+            __threadfence_system();
+            *reinterpret_cast<volatile unsigned *>(&b.done[prev_id]) = 1u;
+        }
         const int qi = ld_relaxed_int(&w.ctl->cur_query);
         if (qi >= b.nq) return;
         const BatchQuery &q = b.queries[qi];
@@ -1830,6 +1836,8 @@ __global__ void __launch_bounds__(kBlock, TRAV_SSSP_MIN_BLOCKS) batch_persistent
             ph = sssp_query(a, sh, defer, ph);
         }
         if (ph < 0) return;
+        if (b.done) __threadfence_system();  // this thread's results, before the next dispatch barrier
+        prev_id = q.id;
     }
 }
 

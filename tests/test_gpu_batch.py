@@ -146,8 +146,8 @@ def test_batch_errors(batch_case):
 
 @pytest.mark.parametrize("parts", [1, 3, 4])
 def test_host_output_batch_equals_device_output_batch(parts):
-    """trav_batch_run_host (host output arrays, shrinking launches with overlapped copies) gives the results
-    of trav_batch_run, and the oracle's."""
+    """trav_batch_run_host (host output arrays; per-query copies started by the kernel's completion flags while
+    the launch runs; one or several launches) gives the results of trav_batch_run, and the oracle's."""
     import torch
 
     s, d, w = O.rmat(12, 16, seed=31)
