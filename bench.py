@@ -186,16 +186,17 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel: str, queries: int = 1):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/traffic.txt), if any.  An entry
-    with bytes_per_query (a capture of fewer queries than the bench's launch) is scaled to `queries`."""
+def ncu_traffic(kernel: str, queries: int = 1, workload: str = ""):
+    """DRAM bytes per launch of `kernel` on `workload` (e.g. rmat_s23_ef32) from the committed ncu summary
+    (profiles/traffic.txt), if any.  An entry with bytes_per_query (a capture of fewer queries than the bench's
+    launch, on the same graph) is scaled to `queries`; an entry for another workload does not count."""
     p = os.path.join(ROOT, "profiles", "traffic.txt")
     if not os.path.exists(p):
         return None
     with open(p) as f:
         for line in f:
             kv = dict(x.split("=", 1) for x in line.split() if "=" in x)
-            if kv.get("kernel") != kernel:
+            if kv.get("kernel") != kernel or kv.get("workload", workload) != workload:
                 continue
             if "bytes_per_launch" in kv:
                 return float(kv["bytes_per_launch"])
@@ -507,7 +508,7 @@ def run_ours(a):
     achieved = launch_bytes / (mean_ms / 1e3) / 1e9
     peak, peak_src = measured_peaks()
     kname = "batch_persistent"
-    traffic = ncu_traffic(kname, queries=len(queries[primary]))
+    traffic = ncu_traffic(kname, queries=len(queries[primary]), workload=f"rmat_s{a.scale}_ef{a.ef}")
 
     if rank == 0:
         per = {names[k]: {"gteps": job_gteps(traversals, E, world, r["ms"] / 1e3), "ms_per_step": r["ms"] / a.steps,
