@@ -515,6 +515,15 @@ __device__ void write_back(const TravArgs &a)
 #ifndef TRAV_BU_LAZY
 #define TRAV_BU_LAZY 1
 #endif
+// SSSP light rounds hold back long light rows more than this many deltas above
+// the frontier's lowest distance while short rows remain (negative: never).
+// Summed over 64-query SSSP batches on four graphs (RMAT s23 ef32, s24 ef16, a
+// flatter RMAT 45/25/15/15, uniform 2^23): 850 ms never, 822 at 0.5, 821 at 1,
+// 841 at 2; the flatter RMAT gains 9%, the others move less than 1%.
+#ifndef TRAV_HOLD_SLACK
+#define TRAV_HOLD_SLACK 1.0f
+#endif
+constexpr float kHoldSlack = TRAV_HOLD_SLACK;
 // Bitmap words a warp works on at once in a bottom-up step.
 #ifndef TRAV_BU_WORDS
 #define TRAV_BU_WORDS 3
@@ -583,6 +592,7 @@ struct CtaCounters {
     unsigned long long mf, scanned;
     unsigned big_total[2];
     int far_key;
+    int light_key;  // SSSP: max of 0x7fffffff - bits(d) over the light frontier pushed (0 = none)
 };
 
 // Destination of one phase's pushes.
@@ -608,6 +618,7 @@ struct Pusher {
     unsigned big_total[2];
     unsigned long long mf, scanned;  // lane-partial sums
     int far_key;                     // lane-partial max
+    int light_key;                   // lane-partial max (SSSP light frontier; see CtaCounters)
 };
 
 // Row part [begin, end) of vertex v.
@@ -636,6 +647,7 @@ __device__ __forceinline__ Pusher make_pusher(const TravArgs &a, const FrontierO
     p.big_total[0] = p.big_total[1] = 0;
     p.mf = p.scanned = 0;
     p.far_key = 0;
+    p.light_key = 0;
     return p;
 }
 
@@ -736,12 +748,14 @@ __device__ void finish_phase(Pusher &p, CtaCounters &cc)
 #pragma unroll
     for (int d = 16; d; d >>= 1) sc += __shfl_xor_sync(kFull, sc, d);
     const int fk = __reduce_max_sync(kFull, p.far_key);
+    const int lk = __reduce_max_sync(kFull, p.light_key);
     if (lane_id() == 0) {
         if (mf) atomicAdd(&cc.mf, mf);
         if (sc) atomicAdd(&cc.scanned, sc);
         if (p.big_total[0]) atomicAdd(&cc.big_total[0], p.big_total[0]);
         if (p.big_total[1]) atomicAdd(&cc.big_total[1], p.big_total[1]);
         if (fk) atomicMax(&cc.far_key, fk);
+        if (lk) atomicMax(&cc.light_key, lk);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -751,9 +765,13 @@ __device__ void finish_phase(Pusher &p, CtaCounters &cc)
         if (cc.big_total[0]) atomicAdd(&sl->big_add, cc.big_total[0]);
         if (cc.big_total[1]) atomicAdd(&sl->hbig_add, cc.big_total[1]);
         if (cc.far_key) atomicMax(&sl->min_far_bits, cc.far_key);
+        // SSSP phases that push a light frontier leave mf (a sum only BFS and
+        // the pull check use) free: it carries the frontier's lowest distance
+        if (cc.light_key) atomicMax(&sl->mf, (unsigned long long)cc.light_key);
         cc.mf = cc.scanned = 0;
         cc.big_total[0] = cc.big_total[1] = 0;
         cc.far_key = 0;
+        cc.light_key = 0;
     }
     // the next phase's pushes are staged only after the grid barrier, which
     // begins with __syncthreads, so the reset is seen before any reuse
@@ -773,8 +791,19 @@ __device__ void expand_frontier(const TravArgs &a, const int32_t *q, unsigned nq
     for (unsigned c = gwarp; c < nch; c += nwarps) {
         const int2 it = chunks[c];
         const int u = it.x, start = it.y;
-        const int end = min(start + a.item, row_part(a, u, kPart).y);
+        const int2 rp = row_part(a, u, kPart);
+        const int end = min(start + a.item, rp.y);
         const float du = vis.begin(u);
+        if (kPart == kPartLight && nq > 0 && vis.hold(du)) {
+            // A long light row (a hub's) whose distance is well above the
+            // frontier's lowest would likely be improved again, and rescanned
+            // in full each time: while short rows are still being expanded it
+            // waits, and the row's first item queues it for the next round.
+            const bool carry = start == rp.x && lane == 0 && vis.stamp_carry(u);
+            push(p, 0, carry, u, (unsigned)a.small_deg + 1u);
+            if (carry) p.light_key = max(p.light_key, 0x7fffffff - __float_as_int(du));
+            continue;
+        }
         if (lane == 0) p.scanned += (unsigned long long)(end - start);
         for (int e0 = start; e0 < end; e0 += 32 * kBatch) {
             int us[kBatch], e[kBatch];
@@ -868,6 +897,8 @@ struct BfsPush {
     int level_next;
 
     __device__ __forceinline__ float begin(int) const { return 0.0f; }
+    __device__ __forceinline__ bool hold(float) const { return false; }
+    __device__ __forceinline__ bool stamp_carry(int) const { return false; }
     __device__ __forceinline__ void finish(Pusher &) const {}
 
     __device__ __forceinline__ void load_at(const int (&e)[kBatch], const bool (&ok)[kBatch], int (&v)[kBatch],
@@ -963,8 +994,28 @@ struct SsspVisit {
     unsigned round;          // id of this round (>= 1)
     unsigned h_start;        // round the current heavy list began in
     unsigned f_start;        // round the current far pile began in
+    float hold_above = INFINITY;  // light rounds: long rows above this distance wait (see expand_frontier)
 
     __device__ __forceinline__ float begin(int u) const { return dist_of(__ldcg(&a->dist[u])); }
+    __device__ __forceinline__ bool hold(float du) const { return du > hold_above; }
+
+    // Queue a held vertex for the next round without a new distance: stamp its
+    // word with this round, keeping the distance and the flags, unless a
+    // relaxation of this round already did (and pushed it).  Either way the
+    // vertex enters the next frontier once.  A frontier vertex's stamp is from
+    // the heavy list's span already, so the heavy-list test reads the same.
+    __device__ __forceinline__ bool stamp_carry(int u) const
+    {
+        unsigned long long w = __ldcg(&a->dist[u]);
+        while (((unsigned)w >> kClsBits) < round) {
+            const unsigned long long nw =
+                (w & ~0xffffffffull) | (unsigned long long)(round << kClsBits | ((unsigned)w & kClsMask));
+            const unsigned long long old = atomicCAS(&a->dist[u], w, nw);
+            if (old == w) return true;
+            w = old;  // lowered (and stamped) meanwhile: look again
+        }
+        return false;
+    }
 
     template <int kPart>
     __device__ __forceinline__ void load_at(const int (&e)[kBatch], const bool (&ok)[kBatch], int (&v)[kBatch],
@@ -1144,6 +1195,7 @@ struct SsspVisit {
         push(p, 0, light, v, cls & kClsLightBig ? big_len : 1u);
         push(p, 1, heavy, v, cls & kClsHeavyBig ? big_len : 1u);
         push_far(p, far, v, far ? 0x7fffffff - __float_as_int(nd) : 0);
+        if (light) p.light_key = max(p.light_key, 0x7fffffff - __float_as_int(nd));
     }
 };
 
@@ -1156,6 +1208,7 @@ __device__ __forceinline__ void init_counters(CtaCounters &cc)
         cc.mf = cc.scanned = 0;
         cc.big_total[0] = cc.big_total[1] = 0;
         cc.far_key = 0;
+        cc.light_key = 0;
     }
     __syncthreads();
 }
@@ -1540,6 +1593,14 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
     }
 
     int steps = 0, buckets = 1;
+    // Light rounds hold back long light rows whose distance is more than
+    // kHoldSlack x delta above the lowest distance of the round's frontier (a
+    // vertex at or below that lowest distance is final: every later candidate
+    // comes from a frontier vertex plus a weight >= 0).
+    float hold_above = INFINITY;
+    auto next_hold = [&](const SlotView &v) {
+        return kHoldSlack >= 0.0f && v.mf ? __int_as_float(0x7fffffff - (int)v.mf) + kHoldSlack * a.delta : INFINITY;
+    };
     while (true) {
         if (steps + buckets >= a.max_steps) {
             if (gtid == 0) atomicCAS(&ctl->err, 0, kErrBudget);
@@ -1557,7 +1618,7 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
                                   (unsigned)far_len,
                                   &ctl->slot[ph % kSlots]};
             Pusher p = make_pusher(a, out, mys, myd);
-            const SsspPush vis{&a, thr, (unsigned)ph, h_start, f_start};
+            const SsspPush vis{&a, thr, (unsigned)ph, h_start, f_start, hold_above};
             if (lpart == kPartLight)
                 expand_frontier<kPartLight>(a, (cur ? a.q1 : a.q0), nq, (cur ? a.chunks1 : a.chunks0), nch, vis, p);
             else
@@ -1567,6 +1628,7 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
             lg.scanned += s_view.scanned;
             log_phase(ctl, lg, 3, nq + nbig);
             const SlotView s0 = s_view;
+            hold_above = next_hold(s0);
             ph++;
             if (gtid == 0 && steps < kMaxTrace) ctl->frontier[steps] = nq + nbig;
             nq = s0.q_add;
@@ -1637,6 +1699,7 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
             lg.scanned += s_view.scanned;
             log_phase(ctl, lg, pull ? 7 : 5, hq + hbig);
             const SlotView s0 = s_view;
+            hold_above = next_hold(s0);
             ph++;
             nq = s0.q_add;
             nch = s0.chunk_add;
@@ -1704,6 +1767,7 @@ __device__ __forceinline__ int sssp_query(const TravArgs &a, QueryShared &sh, De
             lg.scanned += s_view.scanned;
             log_phase(ctl, lg, 4, (unsigned)far_len);
             const SlotView s0 = s_view;
+            hold_above = INFINITY;  // a bucket's first round expands everything it opened with
             ph++;
             nq = s0.q_add;
             nch = s0.chunk_add;
