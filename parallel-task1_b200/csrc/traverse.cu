@@ -516,12 +516,14 @@ __device__ void write_back(const TravArgs &a)
 #define TRAV_BU_LAZY 1
 #endif
 // SSSP light rounds hold back long light rows more than this many deltas above
-// the frontier's lowest distance while short rows remain (negative: never).
-// Summed over 64-query SSSP batches on four graphs (RMAT s23 ef32, s24 ef16, a
-// flatter RMAT 45/25/15/15, uniform 2^23): 850 ms never, 822 at 0.5, 821 at 1,
-// 841 at 2; the flatter RMAT gains 9%, the others move less than 1%.
+// the frontier's lowest distance while short rows remain (negative: never, and
+// none of it is compiled in).  Summed over 64-query SSSP batches on four graphs
+// (RMAT s23 ef32, s24 ef16, a flatter RMAT 45/25/15/15, uniform 2^23): 850 ms
+// never, 822 at 0.5, 821 at 1, 841 at 2 -- the flatter RMAT gains 9% -- but at
+// 1 single queries took 12% longer on RMAT s26 ef16 and 5% longer at s22, so it
+// is off by default.
 #ifndef TRAV_HOLD_SLACK
-#define TRAV_HOLD_SLACK 1.0f
+#define TRAV_HOLD_SLACK -1.0f
 #endif
 constexpr float kHoldSlack = TRAV_HOLD_SLACK;
 // Bitmap words a warp works on at once in a bottom-up step.
@@ -748,7 +750,7 @@ __device__ void finish_phase(Pusher &p, CtaCounters &cc)
 #pragma unroll
     for (int d = 16; d; d >>= 1) sc += __shfl_xor_sync(kFull, sc, d);
     const int fk = __reduce_max_sync(kFull, p.far_key);
-    const int lk = __reduce_max_sync(kFull, p.light_key);
+    const int lk = kHoldSlack >= 0.0f ? __reduce_max_sync(kFull, p.light_key) : 0;
     if (lane_id() == 0) {
         if (mf) atomicAdd(&cc.mf, mf);
         if (sc) atomicAdd(&cc.scanned, sc);
@@ -794,7 +796,7 @@ __device__ void expand_frontier(const TravArgs &a, const int32_t *q, unsigned nq
         const int2 rp = row_part(a, u, kPart);
         const int end = min(start + a.item, rp.y);
         const float du = vis.begin(u);
-        if (kPart == kPartLight && nq > 0 && vis.hold(du)) {
+        if (kHoldSlack >= 0.0f && kPart == kPartLight && nq > 0 && vis.hold(du)) {
             // A long light row (a hub's) whose distance is well above the
             // frontier's lowest would likely be improved again, and rescanned
             // in full each time: while short rows are still being expanded it
@@ -1195,7 +1197,7 @@ struct SsspVisit {
         push(p, 0, light, v, cls & kClsLightBig ? big_len : 1u);
         push(p, 1, heavy, v, cls & kClsHeavyBig ? big_len : 1u);
         push_far(p, far, v, far ? 0x7fffffff - __float_as_int(nd) : 0);
-        if (light) p.light_key = max(p.light_key, 0x7fffffff - __float_as_int(nd));
+        if (kHoldSlack >= 0.0f && light) p.light_key = max(p.light_key, 0x7fffffff - __float_as_int(nd));
     }
 };
 
