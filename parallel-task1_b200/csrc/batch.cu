@@ -161,11 +161,23 @@ int shape_ok(const trav_batch_shape &s, int most)
 bool finite_delta(float d) { return d > 0.0f && std::isfinite(d); }
 
 constexpr int kBusy = 1;  // a run_launch poll's "keep calling me" (TRAV_OK and the errors are <= 0)
+#ifndef TRAV_SMOOTH_ORDER
+#define TRAV_SMOOTH_ORDER 1
+#endif
+constexpr bool kSmoothOrder = TRAV_SMOOTH_ORDER;  // host-output runs spread the cheap queries (build_queries)
 
 // Descriptors in dispatch order: the most edges first (an SSSP query counts
 // as four BFS queries), so the long queries start while the short ones fill
 // the gaps.
-int build_queries(trav_batch *b, const trav_query *qs, int32_t n, std::vector<BatchQuery> *out)
+//
+// With smooth_tail > 0 (host-output runs) the results also have to cross to
+// the host as the queries finish.  Largest first ends with a burst of short
+// queries whose results arrive faster than the copy engine takes them (at RMAT
+// s23: 64 BFS results, 2.1 GB, in the last 24 ms against 57 GB/s).  So the
+// cheaper queries are spread among the expensive ones in proportion, keeping
+// only the smooth_tail cheapest for the end (two per team), where short
+// queries still even out the teams' finishing times.
+int build_queries(trav_batch *b, const trav_query *qs, int32_t n, std::vector<BatchQuery> *out, int smooth_tail = 0)
 {
     std::vector<int32_t> order((size_t)n);
     std::iota(order.begin(), order.end(), 0);
@@ -174,6 +186,25 @@ int build_queries(trav_batch *b, const trav_query *qs, int32_t n, std::vector<Ba
         return (double)(g->g.E + g->g.V) * (qs[i].kind == 1 ? 4.0 : 1.0);
     };
     std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return cost(x) > cost(y); });
+    if (smooth_tail > 0 && n > 0) {
+        double mean = 0.0;
+        for (int32_t i : order) mean += cost(i) / n;
+        std::vector<int32_t> big, small;  // both still most expensive first
+        for (int32_t i : order) (cost(i) > mean ? big : small).push_back(i);
+        const size_t t = std::min(small.size(), (size_t)smooth_tail);
+        const std::vector<int32_t> tail(small.end() - (std::ptrdiff_t)t, small.end());
+        small.resize(small.size() - t);
+        const double per = big.empty() ? 0.0 : (double)small.size() / (double)big.size();
+        double owed = 0.0;
+        size_t si = 0;
+        order.clear();
+        for (int32_t i : big) {
+            order.push_back(i);
+            for (owed += per; si < small.size() && owed >= 1.0; owed -= 1.0) order.push_back(small[si++]);
+        }
+        while (si < small.size()) order.push_back(small[si++]);
+        order.insert(order.end(), tail.begin(), tail.end());
+    }
     out->clear();
     for (int32_t i : order) {
         const trav_query &q = qs[i];
@@ -295,11 +326,11 @@ int run_launch(trav_batch *b, int32_t n, const trav_batch_shape &s, float *ms, u
     return TRAV_OK;
 }
 
-int upload_queries(trav_batch *b, const trav_query *qs, int32_t n)
+int upload_queries(trav_batch *b, const trav_query *qs, int32_t n, int smooth_tail = 0)
 {
     TRY(check_queries_host(b, qs, n));
     std::vector<BatchQuery> d;
-    TRY(build_queries(b, qs, n, &d));
+    TRY(build_queries(b, qs, n, &d, smooth_tail));
     if (n > b->q_cap) {
         TRY_CUDA(cudaStreamSynchronize(b->st));
         cudaFree(b->d_q);
@@ -489,7 +520,9 @@ int trav_batch_run_host(trav_batch *b, const trav_query *queries, int32_t n, int
     for (int p = 0; p < parts; p++) {
         const int32_t q0 = cut[(size_t)p], q1 = cut[(size_t)p + 1];
         if (q1 <= q0) continue;
-        TRY(upload_queries(b, dq.data() + q0, q1 - q0));
+        const int most = persistent_grid_size(2);
+        const int teams = std::max(1, std::min(most > 0 ? most / std::max(1, b->shape.team_ctas) : 1, q1 - q0));
+        TRY(upload_queries(b, dq.data() + q0, q1 - q0, kSmoothOrder ? 2 * teams : 0));
         std::memset(b->done, 0, sizeof(unsigned) * (size_t)(q1 - q0));
         int32_t left = q1 - q0;
         auto poll = [&](bool) -> int {
