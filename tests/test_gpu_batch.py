@@ -181,3 +181,35 @@ def test_host_output_batch_equals_device_output_batch(parts):
     assert T.lib().trav_batch_run_host(b._h, arr, 1, 2, C.byref(ms_out)) == T.TRAV_ERR_BAD_ARG
     b.close()
     g.free()
+
+
+def test_host_output_batch_interleaves_cheap_queries_and_stays_exact():
+    """A host-output batch with few teams spreads its cheap (BFS) queries among the expensive (SSSP) ones and
+    keeps two per team for the end; the results are still the device-output batch's and the oracle's."""
+    import torch
+
+    s, d, w = O.rmat(13, 16, seed=37)
+    V = 1 << 13
+    g = T.Graph.from_edges(V, s, d, w)
+    deg = np.bincount(s, minlength=V)
+    srcs = [int(x) for x in np.flatnonzero(deg > 0)[::97][:20]]
+    dev_q, host_q, host_out = [], [], []
+    for src in srcs:
+        for kind in (1, 0):
+            dt = torch.float32 if kind == 1 else torch.int32
+            dev_q.append((0, kind, src, 0.1, T.SCHEDULE_PLAIN, torch.empty(V, dtype=dt, device="cuda")))
+            h = torch.full((V,), 7, dtype=dt).pin_memory()
+            host_out.append(h)
+            host_q.append((0, kind, src, 0.1, T.SCHEDULE_PLAIN, h))
+    b = T.Batch([g])
+    b.shape = (148, 32, 256)  # four teams: 40 queries, the last 8 BFS, 12 BFS spread among 20 SSSP
+    b.run(dev_q)
+    b.run_host(host_q, parts=1)
+    for (gi, kind, src, _, _, dv), h in zip(dev_q, host_out):
+        assert np.array_equal(h.numpy().view(np.uint32), dv.cpu().numpy().view(np.uint32)), (kind, src)
+        if kind == 1:
+            assert np.array_equal(h.numpy().view(np.uint32), O.bellman_ford(V, s, d, w, src).view(np.uint32))
+        else:
+            assert np.array_equal(h.numpy(), O.bfs_levels(V, s, d, src))
+    b.close()
+    g.free()
