@@ -517,30 +517,37 @@ int trav_batch_run_host(trav_batch *b, const trav_query *queries, int32_t n, int
         return TRAV_OK;
     };
     float total = 0.0f;
-    for (int p = 0; p < parts; p++) {
-        const int32_t q0 = cut[(size_t)p], q1 = cut[(size_t)p + 1];
-        if (q1 <= q0) continue;
-        const int most = persistent_grid_size(2);
-        const int teams = std::max(1, std::min(most > 0 ? most / std::max(1, b->shape.team_ctas) : 1, q1 - q0));
-        TRY(upload_queries(b, dq.data() + q0, q1 - q0, kSmoothOrder ? 2 * teams : 0));
-        std::memset(b->done, 0, sizeof(unsigned) * (size_t)(q1 - q0));
-        int32_t left = q1 - q0;
-        auto poll = [&](bool) -> int {
-            for (int32_t i = q0; i < q1 && left > 0; i++)
-                if (!sent[(size_t)i] && flag[i - q0]) {
-                    TRY(send(i));
-                    left--;
-                }
-            return left > 0 ? kBusy : TRAV_OK;
-        };
-        float ms = 0.0f;
-        TRY(run_launch(b, q1 - q0, b->shape, &ms, done_dev, poll));
-        total += ms;
-        // the launch has ended: whatever was not copied yet goes now
-        for (int32_t i = q0; i < q1; i++)
-            if (!sent[(size_t)i]) TRY(send(i));
-    }
-    TRY_CUDA(cudaStreamSynchronize(b->cst));
+    // Copies may be queued when a launch fails: whatever happens, the call
+    // returns only once none of them can still write the caller's arrays.
+    const int rc = [&]() -> int {
+        for (int p = 0; p < parts; p++) {
+            const int32_t q0 = cut[(size_t)p], q1 = cut[(size_t)p + 1];
+            if (q1 <= q0) continue;
+            const int most = persistent_grid_size(2);
+            const int teams = std::max(1, std::min(most > 0 ? most / std::max(1, b->shape.team_ctas) : 1, q1 - q0));
+            TRY(upload_queries(b, dq.data() + q0, q1 - q0, kSmoothOrder ? 2 * teams : 0));
+            std::memset(b->done, 0, sizeof(unsigned) * (size_t)(q1 - q0));
+            int32_t left = q1 - q0;
+            auto poll = [&](bool) -> int {
+                for (int32_t i = q0; i < q1 && left > 0; i++)
+                    if (!sent[(size_t)i] && flag[i - q0]) {
+                        TRY(send(i));
+                        left--;
+                    }
+                return left > 0 ? kBusy : TRAV_OK;
+            };
+            float ms = 0.0f;
+            TRY(run_launch(b, q1 - q0, b->shape, &ms, done_dev, poll));
+            total += ms;
+            // the launch has ended: whatever was not copied yet goes now
+            for (int32_t i = q0; i < q1; i++)
+                if (!sent[(size_t)i]) TRY(send(i));
+        }
+        return TRAV_OK;
+    }();
+    const cudaError_t ce = cudaStreamSynchronize(b->cst);
+    if (rc != TRAV_OK) return rc;
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamSynchronize(b->cst)");
     if (device_ms) *device_ms = total;
     return TRAV_OK;
 }
