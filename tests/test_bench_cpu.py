@@ -47,3 +47,13 @@ def test_both_arms_print_the_same_config():
     assert c == bench.bench_config(a, 1 << 23, 268431728, 1)
     assert "delta 0.1" in c["workload"] and "delta-stepping" not in c["workload"]
     assert set(bench.host_cpu()) == {"cpu_model", "physical_cores", "logical_cpus"}
+
+
+def test_committed_traffic_is_read_for_its_own_workload_only():
+    """roofline.traffic comes from profiles/traffic.txt: a per-query capture on the bench graph is scaled to the
+    launch's queries, and a workload without a capture gets none (not another graph's figure)."""
+    per_query = bench.ncu_traffic("batch_persistent", queries=1, workload="rmat_s23_ef32")
+    assert per_query and per_query > 1e9
+    assert bench.ncu_traffic("batch_persistent", queries=128, workload="rmat_s23_ef32") == pytest.approx(128 * per_query)
+    assert bench.ncu_traffic("batch_persistent", queries=32, workload="rmat_s26_ef16") is None
+    assert bench.ncu_traffic("no_such_kernel", queries=1, workload="rmat_s23_ef32") is None
