@@ -560,9 +560,11 @@ class Batch:
         _check(lib().trav_batch_run(self._h, arr, n, C.byref(ms)))
         return ms.value
 
-    def run_host(self, queries, parts: int = 4) -> float:
-        """Run queries whose `out` is host memory (pinned tensors or numpy arrays) as `parts` shrinking launches,
-        each part's results copied back while the next part runs; returns the summed device time in ms."""
+    def run_host(self, queries, parts: int = 1) -> float:
+        """Run queries whose `out` is host memory (pinned tensors or numpy arrays; pinned memory lets the copies
+        overlap the work).  Each query's results are copied back as soon as the kernel flags it done, while the
+        launch runs on; `parts` > 1 cuts the queries into that many shrinking launches.  Returns the summed
+        device time in ms."""
         arr, n = self._queries(queries, host=True)
         ms = C.c_float(0.0)
         _check(lib().trav_batch_run_host(self._h, arr, n, parts, C.byref(ms)))
